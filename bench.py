@@ -1,0 +1,336 @@
+"""Benchmark of the FDTD time-step loop on B200 (one JSON line on rank 0).
+
+Workload: the plain-method scaling box (vacuum, 32 seeded dielectric blocks,
+PEC half-wave dipole with a 50-ohm gap source, 8-cell CPML, far-field DFT at
+two frequencies), 512 x 512 x 640 cells by default, FP32 fields with
+material-table coefficients.  One step = one full FDTD time step of that grid
+(H half-step + magnetic CPML, port current, E half-step + electric CPML +
+source, port voltage, running far-field DFT).  The metric is Gcell-updates/s
+= cells x steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (under torchrun) every rank advances its own independent problem
+(seed = 1 + rank; the instances share nothing), the time is the max over ranks
+and the value is the whole-job aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "Gcell-updates/s & time-to-S11 at 0.1 dB: FP32/learned vs FP64 plain, 1 B200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _package():
+    name = "special_topics_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    d = os.path.join(ROOT, "special-topics_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(d, "__init__.py"), submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules[name] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def algorithmic_bytes(p, precision: str) -> dict:
+    """Compulsory DRAM bytes of one H and one E launch: each own-field value read
+    and written once, each other-field value read once, the per-cell coefficient
+    data read once (3 one-byte ids, or 3 FP64 arrays), each Psi element read and
+    written once (plus its CPsi for the per-cell layout)."""
+    sh = p.grid.shapes
+    nH = sum(int(np.prod(sh[c])) for c in ("Hx", "Hy", "Hz"))
+    nE = sum(int(np.prod(sh[c])) for c in ("Ex", "Ey", "Ez"))
+    psi_m = psi_e = 0
+    for f in p.cpml:
+        if f is None:
+            continue
+        n = _psi_sizes(p, f)
+        psi_m += n[0] + n[1]
+        psi_e += n[2] + n[3]
+    # bytes per component value: field word, coefficient data, Psi traffic per Psi element
+    w, coef, psi_w = {"f32-table": (4, 1, 8), "f32": (4, 12, 12), "f64": (8, 24, 24)}[precision]
+    return {"h": nH * (2 * w + coef) + nE * w + psi_m * psi_w,
+            "e": nE * (2 * w + coef) + nH * w + psi_e * psi_w}
+
+
+def _psi_sizes(p, f):
+    g = p.grid
+    nx, ny, nz, nc = g.nx, g.ny, g.nz, f.nc
+    a = "xyz".index(f.face[0])
+    if a == 0:
+        return [nc * (ny + 1) * nz, nc * ny * (nz + 1), nc * ny * (nz + 1), nc * (ny + 1) * nz]
+    if a == 1:
+        return [(nx + 1) * nc * nz, nx * nc * (nz + 1), (nx + 1) * nc * nz, nx * nc * (nz + 1)]
+    return [(nx + 1) * ny * nc, nx * (ny + 1) * nc, nx * (ny + 1) * nc, (nx + 1) * ny * nc]
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = [r.split(",") for r in (getattr(self, "out", "") or "").strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ncu_traffic(workload: str):
+    """dram bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{workload}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_oracle_rate(n=(256, 256, 256), budget_s: float = 15.0) -> dict:
+    """The CPU oracle (C restatement of the reference's FP64 loop, OpenMP over
+    all host cores) on a bounded sample of the scaling-box workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    _package()
+    from special_topics_b200 import workloads
+    scn = workloads.scaling_box(n, seed=1, steps=400)
+    threads = os.cpu_count() or 1
+    o = oracle.Oracle(scn, 400, threads=threads)
+    o.step(2)
+    t = time.perf_counter()
+    o.step(3)
+    per = (time.perf_counter() - t) / 3
+    k = int(max(3, min(390, budget_s / max(per, 1e-6))))
+    t = time.perf_counter()
+    o.step(k)
+    dt = time.perf_counter() - t
+    cells = o.nx * o.ny * o.nz
+    return {"value": cells * k / dt / 1e9, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"scaling box {n[0]}x{n[1]}x{n[2]} ({cells} cells), {k} FP64 steps timed after 5 warm-up steps"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", default="512x512x640")
+    ap.add_argument("--precision", default="f32-table", choices=["f32-table", "f32", "f64"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 side measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    args = ap.parse_args()
+    n = tuple(int(x) for x in args.grid.split("x"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    workload = f"scaling-box-{args.grid}"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = cpu_oracle_rate()
+        line = {"metric": METRIC, "value": base["value"], "unit": "Gcell-updates/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload, "precision": "f64 (reference CPU path)"},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pkg = _package()
+    from special_topics_b200 import workloads
+    from special_topics_b200.backend import Engine
+    from special_topics_b200.scenario import build_problem_from_scenario
+
+    K, W, P = args.steps, args.warmup, 16
+    scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P)
+    t0 = time.perf_counter()
+    prob = build_problem_from_scenario(scn, K + W + P, per_cell=(args.precision != "f32-table"))
+    setup_s = time.perf_counter() - t0
+    cells = prob.grid.cells
+
+    # --- end to end through the C ABI with host buffers: upload + K steps + readback
+    barrier()
+    e2e = None
+    t0 = time.perf_counter()
+    if not args.no_e2e:
+        eng = Engine(prob, args.precision, device=local)
+        h2d = _uploaded_bytes(prob, args.precision)
+        eng.run(K)
+        V, I = eng.voltages(K), eng.currents(K)
+        ff = eng.farfield()
+        e2e_s = time.perf_counter() - t0
+        d2h = sum(v.nbytes for v in V + I) + sum(a[0].nbytes + a[1].nbytes for a in ff.values())
+        eng.close()
+        e2e_s = max_over_ranks(e2e_s)
+        e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+               "note": "one step's share of a whole run through the C ABI: uploads from host buffers, "
+                       "K steps, readback of port traces and far-field accumulators"}
+
+    # --- device-timed run
+    eng = Engine(prob, args.precision, device=local)
+    eng.run(W)
+    barrier()
+    with ClockSampler(local) as clk:
+        ms = eng.run_timed(K)
+    barrier()
+    ms = max_over_ranks(ms)
+    kern = eng.profile_kernels(P)
+    eng.close()
+    value = world * cells * K / (ms / 1e3) / 1e9
+    byts = algorithmic_bytes(prob, args.precision)
+    dom = "e" if kern["e"] >= kern["h"] else "h"
+    peak, peak_kind = hbm_peak()
+    achieved = byts[dom] / (kern[dom] / 1e3) / 1e9
+    traffic = ncu_traffic(workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision != "f64" else "f64",
+        "data": "synthetic (seeded scaling-box scenario in the reference's JSON schema)",
+        "config": {"workload": workload, "cells": cells, "precision": args.precision,
+                   "time_steps_in_problem": K + W + P, "far_field_freqs": 2,
+                   "l2": "inputs larger than L2 (fields and ids >> 126 MB), no flush needed",
+                   "parallelism": f"{world} independent problem(s), one per GPU"},
+        "roofline": {"bound": "hbm", "kernel": f"k_step_{dom}", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom],
+                     "traffic": traffic},
+        "kernel_ms": kern,
+        "clocks": clk.summary(),
+        "gpu_launches": 4 * K,
+        "e2e": e2e,
+        "setup_s": setup_s,
+    }
+    if rank == 0 and world == 1 and not args.no_fp64:
+        line["fp64_plain"] = fp64_side(pkg)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_oracle_rate()
+        except Exception as e:  # the baseline must not hide the GPU number
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _uploaded_bytes(p, precision: str) -> int:
+    b = 0
+    if precision == "f32-table":
+        b += p.meta["material_grid"].nbytes
+    else:
+        b += sum(a.nbytes for a in p.coeffs.values())
+    for f in p.cpml:
+        if f is not None:
+            b += 6 * f.nc * 8 + (sum(c.nbytes for c in f.cpsi) if f.cpsi is not None else 0)
+    for vs in p.voltage_sources:
+        b += vs.field_indices.nbytes + vs.coef.nbytes + vs.voltage_per_e_field.nbytes
+    return b
+
+
+def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
+    """The FP64 drop-in path (reference coefficient layout) on a 256^3 box."""
+    from special_topics_b200 import workloads
+    from special_topics_b200.backend import Engine
+    from special_topics_b200.scenario import build_problem_from_scenario
+    p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=K + W + 8), K + W + 8)
+    eng = Engine(p, "f64")
+    eng.run(W)
+    ms = eng.run_timed(K)
+    kern = eng.profile_kernels(8)
+    eng.close()
+    byts = algorithmic_bytes(p, "f64")
+    peak, _ = hbm_peak()
+    dom = "e" if kern["e"] >= kern["h"] else "h"
+    ach = byts[dom] / (kern[dom] / 1e3) / 1e9
+    return {"workload": f"scaling-box-{n[0]}x{n[1]}x{n[2]}", "value": p.grid.cells * K / (ms / 1e3) / 1e9,
+            "unit": "Gcell-updates/s", "ms_per_step": ms / K,
+            "roofline": {"kernel": f"k_step_{dom}", "achieved": ach, "peak": peak, "frac": ach / peak}}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * fdtd_b200.h -- C ABI of the B200 (sm_100a) FDTD time-step engine.
+ *
+ * Drop-in for the reference's CUDA backend boundary
+ * (js_fdtd/src/backends/cuda/native/fdtd_cuda.h:12-63, driven by
+ * js_fdtd/src/backends/cuda/native/binding.cpp:174-185 and
+ * js_fdtd/src/backends/cuda/cudaBackend.js:183-289).  Every legacy entry point
+ * of that header is exported under the same name and signature; the rest is a
+ * superset: a handle per simulation, FP64 uploads, several sources and probes,
+ * the far-field DFT on the device, material-table (FP32) problems, many
+ * problems advanced in one launch, and watchdog status codes.
+ *
+ * Plain pointers and sizes only.  Host buffers are borrowed for the duration
+ * of a call and copied to the device inside it (binding.cpp:51-60 semantics).
+ * Every call is synchronous with respect to the host; a handle owns one CUDA
+ * stream and must not be used from two host threads at once.
+ *
+ * Index conventions are those of the reference's problem object
+ * (js_fdtd/src/backends/CONTRACT.md:15-57): flat, row-major, 0-based,
+ * k fastest; component extents Hx (nx+1,ny,nz) Hy (nx,ny+1,nz) Hz (nx,ny,nz+1)
+ * Ex (nx,ny+1,nz+1) Ey (nx+1,ny,nz+1) Ez (nx+1,ny+1,nz).
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  FDTD_OK / FDTD_ERR keep the reference's values (fdtd_cuda.h:12-13). */
+#define FDTD_OK 0
+#define FDTD_ERR 1
+#define FDTD_ERR_BADARG 2     /* argument failed validation; nothing was changed */
+#define FDTD_ERR_OOM 3        /* device allocation failed */
+#define FDTD_ERR_CUDA 4       /* a CUDA runtime call failed */
+#define FDTD_ERR_NONFINITE 5  /* the watchdog saw a NaN/Inf port sample; see fdtd_status */
+#define FDTD_ERR_STATE 6      /* call not valid in the handle's current state */
+
+/* Arithmetic of a problem's fields. */
+#define FDTD_PREC_F64 0       /* FP64 fields, 18 per-cell coefficient arrays (the reference's layout) */
+#define FDTD_PREC_F32 1       /* FP32 fields, 18 per-cell coefficient arrays */
+#define FDTD_PREC_F32_TABLE 2 /* FP32 fields, per-component material ids into coefficient tables */
+
+/* Field ids (fdtd_cuda.cu read_field order). */
+#define FDTD_HX 0
+#define FDTD_HY 1
+#define FDTD_HZ 2
+#define FDTD_EX 3
+#define FDTD_EY 4
+#define FDTD_EZ 5
+
+/* Legacy problem size (fdtd_cuda.h:15-19).  Spacings are float there. */
+typedef struct {
+  int nx, ny, nz;
+  float dx, dy, dz, dt;
+  int numberOfTimeSteps;
+} FdtdDims;
+
+/* Problem size with FP64 spacings and the field arithmetic. */
+typedef struct {
+  int nx, ny, nz;
+  double dx, dy, dz, dt;
+  int numberOfTimeSteps;
+  int precision; /* FDTD_PREC_* */
+  int device;    /* CUDA device ordinal */
+} FdtdConfig;
+
+typedef struct fdtd_ctx fdtd_ctx;
+
+/* ---- legacy global-context API (fdtd_cuda.h:21-63), same names and meaning ---- */
+
+/* Last error message of any failing call on this thread (never NULL). fdtd_cuda.h:22 */
+const char* fdtd_last_error(void);
+/* Number of CUDA devices; 0 and FDTD_OK when there is no driver. fdtd_cuda.h:25 */
+int fdtd_device_count(int* count);
+/* Frees any previous global problem and allocates a new FP32 one. fdtd_cuda.h:28 */
+int fdtd_init(const FdtdDims* d);
+/* Uploads coefficient `which` (0..17 in the order of cudaBackend.js:53-60:
+ * Cexe Cexhz Cexhy Ceye Ceyhx Ceyhz Ceze Cezhy Cezhx Chxh Chxey Chxez Chyh Chyez Chyex
+ * Chzh Chzex Chzey). fdtd_cuda.h:31 */
+int fdtd_upload_coeff(int which, const float* host, int n);
+/* One CPML face, faceId 0..5 = xn xp yn yp zn zp; slots as cudaBackend.js:76-116
+ * (x: hyx hzx eyx ezx, y: hxy hzy ezy exy, z: hxz hyz exz eyz). fdtd_cuda.h:36 */
+int fdtd_upload_cpml(int faceId, int nc, const float* b_e, const float* a_e, const float* b_m,
+                     const float* a_m, const float* CPsi0, int n0, const float* CPsi1, int n1,
+                     const float* CPsi2, int n2, const float* CPsi3, int n3, int m_start, int e_start,
+                     int ascending);
+/* Adds a lumped voltage source (dir 0=x 1=y 2=z). fdtd_cuda.h:43 */
+int fdtd_upload_vsource(int dir, const int* idx, const float* coef, int count, const float* waveform,
+                        int nSteps);
+/* Adds a sampled-voltage probe V = Csvf * sum E[idx]. fdtd_cuda.h:47 */
+int fdtd_upload_svoltage(int dir, const int* idx, int count, float Csvf);
+/* Adds a sampled-current probe as three weighted gather lists. fdtd_cuda.h:50 */
+int fdtd_upload_scurrent(const int* hxIdx, const float* hxW, int hxN, const int* hyIdx, const float* hyW,
+                         int hyN, const int* hzIdx, const float* hzW, int hzN);
+/* Runs steps [tsStart, tsStart+count); svOut/siOut (may be NULL) receive the
+ * first voltage / current probe per step. fdtd_cuda.h:57 */
+int fdtd_run_batch(int tsStart, int count, float* svOut, float* siOut);
+/* Copies field `which` (0=Hx..5=Ez) to the host. fdtd_cuda.h:60 */
+int fdtd_read_field(int which, float* host, int n);
+/* Frees the global problem. fdtd_cuda.h:63 */
+void fdtd_destroy(void);
+
+/* ---- handle API (superset) ---- */
+
+/* Allocates a problem on cfg->device.  Fields, Psi and accumulators start at zero. */
+int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out);
+/* Frees everything the handle owns; NULL is ignored. */
+void fdtd_free(fdtd_ctx* ctx);
+
+/* FP64 / FP32 per-cell coefficient array `which` (same ids as fdtd_upload_coeff).
+ * The host array is FP64 and is rounded once when the problem is FP32. */
+int fdtd_ctx_upload_coeff(fdtd_ctx* ctx, int which, const double* host, long n);
+
+/* One CPML face (js_fdtd/src/cpml.js:147-448): 1-D b/a profiles of length nc,
+ * CPsi slot arrays in the reference's Psi layouts, and the first H / E index of
+ * the face along its axis.  kappa_e / kappa_m (length nc, may be NULL for the
+ * per-cell problems) are needed by FDTD_PREC_F32_TABLE problems, whose
+ * coefficient tables carry no kappa division. */
+int fdtd_ctx_upload_cpml(fdtd_ctx* ctx, int faceId, int nc, const double* b_e, const double* a_e,
+                         const double* b_m, const double* a_m, const double* kappa_e, const double* kappa_m,
+                         const double* CPsi0, long n0, const double* CPsi1, long n1, const double* CPsi2,
+                         long n2, const double* CPsi3, long n3, int m_start, int e_start);
+
+/* Lumped voltage source (sources.js:271-288): E_dir[idx[n]] += coef[n] * wave[ts]
+ * after the electric CPML.  idx must list an axis-aligned box of cells of
+ * component dir in the reference's createLinearIndexList order (k outer, j,
+ * i inner); wave has one value per step (voltage_per_e_field). */
+int fdtd_ctx_add_vsource(fdtd_ctx* ctx, int dir, const int* idx, const double* coef, int count,
+                         const double* wave, int nSteps);
+
+/* Sampled voltage (sampling.js:295-307): V[ts] = Csvf * (sum over idx in order). */
+int fdtd_ctx_add_svoltage(fdtd_ctx* ctx, int dir, const int* idx, int count, double Csvf);
+
+/* Sampled current (sampling.js:204-245) as ONE ordered gather list:
+ * I[ts] = sum_n w[n] * H_comp[n][idx[n]], summed in list order from zero, with
+ * comp 0=Hx 1=Hy 2=Hz and the reference's signs folded into w. */
+int fdtd_ctx_add_scurrent(fdtd_ctx* ctx, const int* comp, const int* idx, const double* w, int count);
+
+/* Running NF-FF DFT on the Huygens box (farfield.js:28-78,90-248).  li..uk are
+ * the reference's 1-based box bounds.  Phasors cos/-sin of w*dt*(ts+0.5) and
+ * w*dt*(ts+1) are evaluated here in FP64, w = 2*pi*f. */
+int fdtd_ctx_setup_farfield(fdtd_ctx* ctx, int nFreq, const double* freqs, int li, int lj, int lk, int ui,
+                            int uj, int uk);
+
+/* Material-table problem (FDTD_PREC_F32_TABLE): one uint8 id per cell and
+ * component selects a row of that component's coefficient table
+ * (rows x 3: self, first curl, second curl coefficient, all without kappa).
+ * comp order Ex Ey Ez Hx Hy Hz; curl order as the per-cell arrays
+ * (Ex: Cexe Cexhz Cexhy, ..., Hz: Chzh Chzex Chzey). */
+int fdtd_ctx_upload_material(fdtd_ctx* ctx, int comp, const unsigned char* ids, long n, const double* table,
+                             int rows);
+
+/* Material-table problem built on the device from the material grid
+ * (materials.js:21-332 + coefficients.js:22-116): `mat` holds one type id per
+ * cell (nx*ny*nz, k fastest; 1-based ids as materials.js stores them), `props`
+ * has 4 values per type id 0..ntypes-1 (eps_r, mu_r, sigma_e, sigma_m, with
+ * materials.js:96-101's zero replacements already applied), `plates` has 7 ints
+ * per zero-thickness PEC plate box (component 0=Ex 1=Ey 2=Ez, then inclusive
+ * i0 i1 j0 j1 k0 k1 of that component array) applied in order with conductivity
+ * plate_sigma[q] (materials.js:253-332).  At most 48 type ids and 64 plates. */
+int fdtd_ctx_build_material(fdtd_ctx* ctx, const unsigned char* mat, long ncells, int ntypes, const double* props,
+                            int nplates, const int* plates, const double* plate_sigma);
+
+/* Gives `count` cells of component comp (API order Ex Ey Ez Hx Hy Hz) their own
+ * coefficient triples (self, curl1, curl2), e.g. the lumped-source cells of
+ * coefficients.js:158-207. */
+int fdtd_ctx_override_material(fdtd_ctx* ctx, int comp, const int* idx, const double* triples, int count);
+
+/* Reads back a component's ids and its coefficient table (FP64, rows x 3). */
+int fdtd_ctx_read_material(fdtd_ctx* ctx, int comp, unsigned char* ids, long n, double* table, int* rows);
+
+/* Runs `count` steps from the handle's current step.  Checks the watchdog at
+ * the end and returns FDTD_ERR_NONFINITE if a port sample went non-finite. */
+int fdtd_ctx_run(fdtd_ctx* ctx, int count);
+/* fdtd_ctx_run that also reports the device time (ms) between CUDA events
+ * recorded on the handle's stream before the first and after the last launch. */
+int fdtd_ctx_run_timed(fdtd_ctx* ctx, int count, float* ms);
+/* Runs `count` steps one at a time with CUDA events around every launch and
+ * returns the mean duration (ms) of the H, mid-step, E and epilogue kernels. */
+int fdtd_ctx_profile_kernels(fdtd_ctx* ctx, int count, double* avg_ms);
+/* Current step index (number of completed steps). */
+int fdtd_ctx_step(const fdtd_ctx* ctx);
+/* Watchdog: *code = FDTD_OK or FDTD_ERR_NONFINITE, *step = first bad step or -1. */
+int fdtd_status(fdtd_ctx* ctx, int* code, int* step);
+
+/* Whole probe traces, FP64, one value per step (first `n` steps). kind 0 = voltage, 1 = current. */
+int fdtd_ctx_read_trace(fdtd_ctx* ctx, int kind, int probe, double* out, int n);
+/* Field `which` as FP64 (FP32 problems are widened). */
+int fdtd_ctx_read_field(fdtd_ctx* ctx, int which, double* host, long n);
+/* CPML Psi slot of a face, as FP64. */
+int fdtd_ctx_read_psi(fdtd_ctx* ctx, int faceId, int slot, double* host, long n);
+/* Far-field accumulator `array` (0..23 in the order cjyxp cjzxp cjyxn cjzxn cjxyp cjzyp
+ * cjxyn cjzyn cjxzp cjyzp cjxzn cjyzn cmyxp cmzxp cmyxn cmzxn cmxyp cmzyp cmxyn cmzyn
+ * cmxzp cmyzp cmxzn cmyzn), laid out [freq][point] like farfield.js:55. */
+int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, long n);
+
+/* Direct time-to-frequency transform on the device (dft.js:17-38):
+ * X(f) = dt * sum_n x[n] exp(-j 2 pi f ((n+1) dt + shift)), FP64. */
+int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,
+             double* im);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDTD_B200_H */

@@ -1,0 +1,241 @@
+"""The B200 backend behind the reference's backend contract.
+
+Mirrors js_fdtd/src/backends/CONTRACT.md:104-137 and the CUDA backend driver
+js_fdtd/src/backends/cuda/cudaBackend.js:165-306: an object with ``name``,
+``is_available()`` (never raises) and ``run(problem)``, a generator that
+advances the whole time loop on the GPU, yields a progress snapshot every
+``batch_size`` steps and on the last step, and leaves the port traces and
+far-field accumulators filled in (``Engine.voltages()`` ... ``farfield()``).
+
+``Engine`` is the handle-level API: it uploads a ``scenario.Problem`` through
+the C ABI (include/fdtd_b200.h) and exposes the device state for checks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from typing import Iterator
+
+import numpy as np
+
+from . import _native as N
+from .scenario import COEFF_ORDER, FF_NAMES, Problem
+from .tables import COMPONENTS, build_tables, check_source_outside_cpml
+
+PRECISIONS = {"f64": N.PREC_F64, "f32": N.PREC_F32, "f32-table": N.PREC_F32_TABLE}
+FIELD_IDS = {"Hx": 0, "Hy": 1, "Hz": 2, "Ex": 3, "Ey": 4, "Ez": 5}
+
+
+class Engine:
+    """One problem resident on one GPU."""
+
+    def __init__(self, problem: Problem, precision: str = "f64", device: int = 0, host_tables: bool = False):
+        """host_tables=True builds an FP32-table problem's ids with numpy
+        (tables.build_tables, needs per-cell material arrays) instead of on the
+        device (fdtd_ctx_build_material)."""
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        L = N.lib()
+        self.problem = problem
+        self.precision = precision
+        self.host_tables = host_tables
+        g = problem.grid
+        cfg = N.FdtdConfig(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.dt, g.numberOfTimeSteps,
+                           PRECISIONS[precision], device)
+        h = C.c_void_p()
+        N.check(L.fdtd_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        try:
+            self._upload()
+        except Exception:
+            self.close()
+            raise
+
+    # -- upload -------------------------------------------------------------
+    def _upload(self) -> None:
+        L, p, h = N.lib(), self.problem, self._h
+        table = self.precision == "f32-table"
+        if table and self.host_tables:
+            for comp_id, (ids, tab) in enumerate(build_tables(p)[c] for c in COMPONENTS):
+                N.check(L.fdtd_ctx_upload_material(h, comp_id, ids.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                                   ids.size, N.dptr(tab.ravel()), tab.shape[0]))
+        elif table:
+            self._build_tables_on_device()
+        else:
+            for w, name in enumerate(COEFF_ORDER):
+                a = np.ascontiguousarray(p.coeffs[name], dtype=np.float64)
+                N.check(L.fdtd_ctx_upload_coeff(h, w, N.dptr(a), a.size))
+        for fid, f in enumerate(p.cpml):
+            if f is None:
+                continue
+            prof = [np.ascontiguousarray(x, dtype=np.float64)
+                    for x in (f.b_e, f.a_e, f.b_m, f.a_m, f.kappa_e, f.kappa_m)]
+            args = []
+            for cp in (f.cpsi if not table else [None] * 4):
+                if cp is None:
+                    args += [None, 0]
+                else:
+                    cp = np.ascontiguousarray(cp, dtype=np.float64)
+                    args += [N.dptr(cp), cp.size]
+            N.check(L.fdtd_ctx_upload_cpml(h, fid, f.nc, *[N.dptr(x) for x in prof], *args, f.m_start, f.e_start))
+        for vs in p.voltage_sources:
+            fi = np.ascontiguousarray(vs.field_indices, dtype=np.int32)
+            cs = np.ascontiguousarray(vs.coef, dtype=np.float64)
+            wv = np.ascontiguousarray(vs.voltage_per_e_field, dtype=np.float64)
+            N.check(L.fdtd_ctx_add_vsource(h, vs.axis, N.iptr(fi), N.dptr(cs), fi.size, N.dptr(wv), wv.size))
+        for sv in p.sampled_voltages:
+            fi = np.ascontiguousarray(sv.field_indices, dtype=np.int32)
+            N.check(L.fdtd_ctx_add_svoltage(h, sv.axis, N.iptr(fi), fi.size, sv.Csvf))
+        for si in p.sampled_currents:
+            comp = np.ascontiguousarray(si.comp, dtype=np.int32)
+            idx = np.ascontiguousarray(si.idx, dtype=np.int32)
+            w = np.ascontiguousarray(si.w, dtype=np.float64)
+            N.check(L.fdtd_ctx_add_scurrent(h, N.iptr(comp), N.iptr(idx), N.dptr(w), comp.size))
+        ff = p.farfield
+        if ff is not None and ff.nFreq > 0:
+            fr = np.ascontiguousarray(ff.frequencies, dtype=np.float64)
+            N.check(L.fdtd_ctx_setup_farfield(h, fr.size, N.dptr(fr), ff.li, ff.lj, ff.lk, ff.ui, ff.uj, ff.uk))
+
+    def _build_tables_on_device(self) -> None:
+        L, p, h = N.lib(), self.problem, self._h
+        mat = np.ascontiguousarray(p.meta["material_grid"], dtype=np.uint8).ravel()
+        props = np.ascontiguousarray(p.meta["material_props"], dtype=np.float64)
+        plates = p.meta["plates"]
+        pl = np.ascontiguousarray(np.array([b[:7] for b in plates], dtype=np.int32).reshape(-1))
+        ps = np.ascontiguousarray(np.array([b[7] for b in plates], dtype=np.float64))
+        N.check(L.fdtd_ctx_build_material(h, mat.ctypes.data_as(C.POINTER(C.c_ubyte)), mat.size, props.shape[0],
+                                          N.dptr(props.reshape(-1)), len(plates), N.iptr(pl), N.dptr(ps)))
+        for vs in p.voltage_sources:
+            check_source_outside_cpml(vs, p)
+            fi = np.ascontiguousarray(vs.field_indices, dtype=np.int32)
+            trip = np.ascontiguousarray(vs.override, dtype=np.float64).reshape(-1)
+            N.check(L.fdtd_ctx_override_material(h, vs.axis, N.iptr(fi), N.dptr(trip), fi.size))
+
+    def material(self, comp: str) -> tuple[np.ndarray, np.ndarray]:
+        """(ids, FP64 table rows x 3) of a table problem's component."""
+        n = int(np.prod(self.problem.grid.shapes[comp]))
+        ids = np.zeros(n, dtype=np.uint8)
+        tab = np.zeros(256 * 3)
+        rows = C.c_int()
+        N.check(N.lib().fdtd_ctx_read_material(self._h, COMPONENTS.index(comp), ids.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                               n, N.dptr(tab), C.byref(rows)))
+        return ids, tab[:3 * rows.value].reshape(-1, 3)
+
+    # -- stepping -------------------------------------------------------------
+    @property
+    def step(self) -> int:
+        return N.lib().fdtd_ctx_step(self._h)
+
+    def run(self, count: int) -> None:
+        N.check(N.lib().fdtd_ctx_run(self._h, int(count)))
+
+    def run_timed(self, count: int) -> float:
+        """Runs `count` steps; returns their device time in ms (CUDA events on the engine's stream)."""
+        ms = C.c_float()
+        N.check(N.lib().fdtd_ctx_run_timed(self._h, int(count), C.byref(ms)))
+        return ms.value
+
+    def profile_kernels(self, count: int) -> dict:
+        """Mean device ms of each kernel over `count` steps run one launch at a time."""
+        out = np.zeros(4)
+        N.check(N.lib().fdtd_ctx_profile_kernels(self._h, int(count), N.dptr(out)))
+        return dict(zip(("h", "mid", "e", "epilogue"), out.tolist()))
+
+    def status(self) -> tuple[int, int]:
+        code, step = C.c_int(), C.c_int()
+        N.check(N.lib().fdtd_status(self._h, C.byref(code), C.byref(step)))
+        return code.value, step.value
+
+    # -- readback -------------------------------------------------------------
+    def _trace(self, kind: int, q: int, n: int | None) -> np.ndarray:
+        n = self.step if n is None else n
+        out = np.zeros(n)
+        N.check(N.lib().fdtd_ctx_read_trace(self._h, kind, q, N.dptr(out), n))
+        return out
+
+    def voltages(self, n: int | None = None) -> list:
+        return [self._trace(0, q, n) for q in range(len(self.problem.sampled_voltages))]
+
+    def currents(self, n: int | None = None) -> list:
+        return [self._trace(1, q, n) for q in range(len(self.problem.sampled_currents))]
+
+    def field(self, name: str) -> np.ndarray:
+        shape = self.problem.grid.shapes[name]
+        out = np.zeros(int(np.prod(shape)))
+        N.check(N.lib().fdtd_ctx_read_field(self._h, FIELD_IDS[name], N.dptr(out), out.size))
+        return out
+
+    def psi(self, face: int, slot: int, n: int) -> np.ndarray:
+        out = np.zeros(n)
+        N.check(N.lib().fdtd_ctx_read_psi(self._h, face, slot, N.dptr(out), n))
+        return out
+
+    def farfield(self) -> dict[str, tuple[np.ndarray, np.ndarray]]:
+        ff = self.problem.farfield
+        if ff is None:
+            return {}
+        ni, nj, nk = ff.ui - ff.li, ff.uj - ff.lj, ff.uk - ff.lk
+        sizes = (nj * nk, ni * nk, ni * nj)
+        out = {}
+        for a, name in enumerate(FF_NAMES):
+            n = ff.nFreq * sizes[(a % 12) // 4]
+            re, im = np.zeros(n), np.zeros(n)
+            N.check(N.lib().fdtd_ctx_read_farfield(self._h, a, N.dptr(re), N.dptr(im), n))
+            out[name] = (re, im)
+        return out
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.lib().fdtd_free(h)
+        self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class B200Backend:
+    """Backend object of the reference's registry contract (CONTRACT.md:121-137)."""
+
+    name = "b200"
+
+    def __init__(self, precision: str = "f64", device: int = 0):
+        self.precision = precision
+        self.device = device
+        self.engine: Engine | None = None
+
+    def is_available(self) -> bool:
+        try:
+            return N.device_count() > 0
+        except Exception:
+            return False
+
+    def meta(self) -> dict:
+        return {"name": self.name, "precision": self.precision, "farfield": "device"}
+
+    def run(self, problem: Problem, batch_size: int = 50) -> Iterator[dict]:
+        g = problem.grid
+        total = g.numberOfTimeSteps
+        eng = Engine(problem, self.precision, self.device)
+        self.engine = eng
+        t0 = time.time()
+        ts = 0
+        while ts < total:
+            n = min(batch_size, total - ts)
+            eng.run(n)
+            ts += n
+            v = None
+            if problem.sampled_voltages:
+                v = float(eng._trace(0, 0, ts)[ts - 1])
+            yield {"step": ts, "total": total, "elapsed": time.time() - t0,
+                   "percent": f"{ts / total * 100:.1f}", "voltage": v,
+                   "time_ns": (ts - 1 + 0.5) * g.dt * 1e9, "backend": self.name}

@@ -1,0 +1,1221 @@
+// fdtd_b200.cu -- host side of the C ABI declared in include/fdtd_b200.h:
+// problem handles, uploads with validation, the per-step launch sequence
+// (captured into a CUDA graph per batch of steps), readbacks and the legacy
+// global-context entry points of js_fdtd/src/backends/cuda/native/fdtd_cuda.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "fdtd_common.cuh"
+#include "fdtd_material.cuh"
+#include "fdtd_step.cuh"
+
+#include <map>
+#include <utility>
+
+using namespace fdtd;
+
+static thread_local char g_err[512] = "no error";
+
+static int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(FDTD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+struct HostFace {
+  bool present = false;
+  int nc = 0, m_start = 0, e_start = 0;
+  void* prof[4] = {};   // b_e a_e b_m a_m (field type)
+  float* inv_k[2] = {};  // 1/kappa_e, 1/kappa_m (table problems)
+  void* psi[4] = {};
+  void* cpsi[4] = {};
+  long long n[4] = {};
+};
+
+struct HostSource {
+  SourceBox box;
+  int count;
+  void* cs;
+  void* wave;
+};
+
+struct HostVProbe {
+  int comp, count;
+  int* idx;
+  double csvf;
+};
+
+struct HostIProbe {
+  int count;
+  int* comp;
+  int* idx;
+  double* w;
+};
+
+}  // namespace
+
+struct fdtd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int prec = FDTD_PREC_F64;
+  size_t esz = 8;  // bytes per field value
+  int nx = 0, ny = 0, nz = 0, nsteps = 0;
+  double dx = 0, dy = 0, dz = 0, dt = 0;
+  int ts = 0;  // completed steps
+  long long ncomp[6] = {};  // Hx Hy Hz Ex Ey Ez element counts
+  void* fields = nullptr;   // contiguous Hx..Ez (+ slack)
+  void* coef[18] = {};
+  bool coef_set[18] = {};
+  // material-table problem
+  unsigned char* ids[6] = {};
+  bool ids_set[6] = {};
+  std::vector<float> table[6];
+  std::vector<double> rows64[6];  // the same rows in FP64 (rows x 3), for overrides and readback
+  float* d_tab = nullptr;      // [6][kTableRows][3], field order
+  float* d_invk[6] = {};       // 1/kappa per axis position: E x y z, H x y z
+  bool table_dirty = true;
+  TableCoef tcoef{};
+  HostFace face[6];
+  std::vector<HostSource> src;
+  std::vector<HostVProbe> vprobe;
+  std::vector<HostIProbe> iprobe;
+  double* V = nullptr;  // traces
+  double* I = nullptr;
+  int nv_alloc = -1, ni_alloc = -1;
+  // far field
+  int nFreq = 0;
+  int li = 0, lj = 0, lk = 0, ui = 0, uj = 0, uk = 0;
+  double* ph = nullptr;
+  double* acc = nullptr;
+  long long ffsz[3] = {};
+  long long ffoff[24] = {};
+  void* ex0b = nullptr;
+  int* d_ts = nullptr;
+  int* d_status = nullptr;
+  // graph cache
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  bool dirty = true;
+  std::vector<void*> owned;  // every device allocation
+};
+
+namespace {
+
+int dalloc(fdtd_ctx* c, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(FDTD_ERR_OOM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  c->owned.push_back(*p);
+  // Zero on the handle's stream and wait: later uploads may use either stream,
+  // and the zeroing must not land after them.
+  e = cudaMemsetAsync(*p, 0, bytes, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "zeroing a new buffer: %s", cudaGetErrorString(e));
+  return FDTD_OK;
+}
+
+void dfree(fdtd_ctx* c, void* p) {
+  if (!p) return;
+  auto it = std::find(c->owned.begin(), c->owned.end(), p);
+  if (it != c->owned.end()) c->owned.erase(it);
+  cudaFree(p);
+}
+
+// Host FP64 array -> device array of the problem's field type.
+int upload_real(fdtd_ctx* c, void* dst, const double* src, long long n) {
+  if (n <= 0) return FDTD_OK;
+  if (c->esz == 8) {
+    CK(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    std::vector<float> tmp(n);
+    for (long long q = 0; q < n; q++) tmp[q] = (float)src[q];
+    CK(cudaMemcpyAsync(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return FDTD_OK;
+}
+
+int read_real(fdtd_ctx* c, const void* srcdev, double* dst, long long n) {
+  if (n <= 0) return FDTD_OK;
+  if (c->esz == 8) {
+    CK(cudaMemcpyAsync(dst, srcdev, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  } else {
+    std::vector<float> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), srcdev, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long q = 0; q < n; q++) dst[q] = tmp[q];
+  }
+  return FDTD_OK;
+}
+
+// Coefficient id -> (component, count) in cudaBackend.js:53-60 order.
+long long coef_count(const fdtd_ctx* c, int which) {
+  static const int comp_of[18] = {3, 3, 3, 4, 4, 4, 5, 5, 5, 0, 0, 0, 1, 1, 1, 2, 2, 2};
+  return c->ncomp[comp_of[which]];
+}
+
+void* field_ptr(const fdtd_ctx* c, int which) {
+  char* base = (char*)c->fields;
+  long long off = 0;
+  for (int q = 0; q < which; q++) off += c->ncomp[q];
+  return base + off * c->esz;
+}
+
+// Expected Psi slot sizes (cpml.js:147-448) for face f with nc cells.
+void psi_sizes(const fdtd_ctx* c, int f, int nc, long long out[4]) {
+  const long long nx = c->nx, ny = c->ny, nz = c->nz, X = nx + 1, Y = ny + 1, Z = nz + 1;
+  if (f / 2 == 0) {
+    out[0] = nc * Y * nz; out[1] = nc * ny * Z; out[2] = nc * ny * Z; out[3] = nc * Y * nz;
+  } else if (f / 2 == 1) {
+    out[0] = X * nc * nz; out[1] = nx * nc * Z; out[2] = X * nc * nz; out[3] = nx * nc * Z;
+  } else {
+    out[0] = X * ny * nc; out[1] = nx * Y * nc; out[2] = nx * Y * nc; out[3] = X * ny * nc;
+  }
+}
+
+void invalidate(fdtd_ctx* c) {
+  c->dirty = true;
+  c->table_dirty = true;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_steps = 0;
+  }
+}
+
+template <typename T>
+Face<T> dev_face(const HostFace& h) {
+  Face<T> f{};
+  if (!h.present) return f;
+  f.nc = h.nc;
+  f.m_start = h.m_start;
+  f.e_start = h.e_start;
+  f.b_e = (const T*)h.prof[0];
+  f.a_e = (const T*)h.prof[1];
+  f.b_m = (const T*)h.prof[2];
+  f.a_m = (const T*)h.prof[3];
+  f.inv_ke = h.inv_k[0];
+  f.inv_km = h.inv_k[1];
+  for (int s = 0; s < 4; s++) {
+    f.psi[s] = (T*)h.psi[s];
+    f.cpsi[s] = (const T*)h.cpsi[s];
+  }
+  return f;
+}
+
+template <typename T>
+Fields<T> dev_fields(const fdtd_ctx* c) {
+  Fields<T> f;
+  f.Hx = (T*)field_ptr(c, 0);
+  f.Hy = (T*)field_ptr(c, 1);
+  f.Hz = (T*)field_ptr(c, 2);
+  f.Ex = (T*)field_ptr(c, 3);
+  f.Ey = (T*)field_ptr(c, 4);
+  f.Ez = (T*)field_ptr(c, 5);
+  return f;
+}
+
+template <typename T>
+Sources<T> dev_sources(const fdtd_ctx* c) {
+  Sources<T> s{};
+  s.n = (int)c->src.size();
+  for (int q = 0; q < s.n; q++) {
+    s.box[q] = c->src[q].box;
+    s.cs[q] = (const T*)c->src[q].cs;
+    s.wave[q] = (const T*)c->src[q].wave;
+  }
+  return s;
+}
+
+Probes dev_probes(const fdtd_ctx* c) {
+  Probes p{};
+  p.n_v = (int)c->vprobe.size();
+  p.n_i = (int)c->iprobe.size();
+  for (int q = 0; q < p.n_v; q++) {
+    p.v_comp[q] = c->vprobe[q].comp;
+    p.v_count[q] = c->vprobe[q].count;
+    p.v_idx[q] = c->vprobe[q].idx;
+    p.v_csvf[q] = c->vprobe[q].csvf;
+  }
+  for (int q = 0; q < p.n_i; q++) {
+    p.i_count[q] = c->iprobe[q].count;
+    p.i_comp[q] = c->iprobe[q].comp;
+    p.i_idx[q] = c->iprobe[q].idx;
+    p.i_w[q] = c->iprobe[q].w;
+  }
+  p.V = c->V;
+  p.I = c->I;
+  p.nsteps = c->nsteps;
+  p.status = c->d_status;
+  return p;
+}
+
+FarField dev_ff(const fdtd_ctx* c) {
+  FarField ff{};
+  ff.nFreq = c->nFreq;
+  if (c->nFreq == 0) return ff;
+  ff.LI = c->li - 1; ff.LJ = c->lj - 1; ff.LK = c->lk - 1;
+  ff.UI = c->ui - 1; ff.UJ = c->uj - 1; ff.UK = c->uk - 1;
+  ff.ni = c->ui - c->li; ff.nj = c->uj - c->lj; ff.nk = c->uk - c->lk;
+  ff.ph = c->ph;
+  ff.acc = c->acc;
+  for (int a = 0; a < 24; a++) ff.off[a] = c->ffoff[a];
+  for (int a = 0; a < 3; a++) ff.sz[a] = c->ffsz[a];
+  return ff;
+}
+
+// Trace buffers follow the probe counts.
+int ensure_traces(fdtd_ctx* c) {
+  const int nv = (int)c->vprobe.size(), ni = (int)c->iprobe.size();
+  if (nv != c->nv_alloc) {
+    dfree(c, c->V);
+    c->V = nullptr;
+    int rc = dalloc(c, (void**)&c->V, sizeof(double) * std::max(nv, 1) * (size_t)c->nsteps);
+    if (rc) return rc;
+    c->nv_alloc = nv;
+  }
+  if (ni != c->ni_alloc) {
+    dfree(c, c->I);
+    c->I = nullptr;
+    int rc = dalloc(c, (void**)&c->I, sizeof(double) * std::max(ni, 1) * (size_t)c->nsteps);
+    if (rc) return rc;
+    c->ni_alloc = ni;
+  }
+  return FDTD_OK;
+}
+
+int check_ready(fdtd_ctx* c) {
+  if (c->prec == FDTD_PREC_F32_TABLE) {
+    for (int q = 0; q < 6; q++)
+      if (!c->ids_set[q]) return fail(FDTD_ERR_STATE, "material ids of component %d not uploaded", q);
+  } else {
+    for (int q = 0; q < 18; q++)
+      if (!c->coef_set[q]) return fail(FDTD_ERR_STATE, "coefficient array %d not uploaded", q);
+  }
+  return FDTD_OK;
+}
+
+// Kernel parameters shared by both coefficient layouts.
+template <typename T, class C>
+StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
+  StepParams<T, C> p{};
+  p.g = GridDims{c->nx, c->ny, c->nz};
+  p.f = dev_fields<T>(c);
+  p.coef = coef;
+  for (int q = 0; q < 6; q++) p.face[q] = dev_face<T>(c->face[q]);
+  p.ex0b = (T*)c->ex0b;
+  p.ts = c->d_ts;
+  p.src = dev_sources<T>(c);
+  p.dcell[0] = (T)c->dx;
+  p.dcell[1] = (T)c->dy;
+  p.dcell[2] = (T)c->dz;
+  return p;
+}
+
+// Per-kernel timing of a profiled run: events around each launch.
+struct KernelTimer {
+  cudaEvent_t ev[5];
+  double ms[4] = {0, 0, 0, 0};
+};
+
+// Enqueue `count` steps on the handle's stream (with `tm`, one step at a time,
+// timing each kernel).
+template <typename T, class C, bool EXACT>
+int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullptr) {
+  StepParams<T, C> p = step_params<T, C>(c, coef);
+  Probes pr = dev_probes(c);
+  FarField ff = dev_ff(c);
+  const dim3 blk(32, 4, 2);
+  const dim3 grd((c->nz + 1 + 31) / 32, (c->ny + 1 + 3) / 4, (c->nx + 1 + 1) / 2);
+  const long long plane = (long long)c->ny * (c->nz + 1);
+  const unsigned mid_blocks = (unsigned)((plane + pr.n_i + 255) / 256);
+  const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
+  const unsigned epi_blocks = (unsigned)((nff + pr.n_v + 255) / 256);
+  for (int s = 0; s < count; s++) {
+    if (tm) CK(cudaEventRecord(tm->ev[0], c->stream));
+    k_step_h<T, C, EXACT><<<grd, blk, 0, c->stream>>>(p);
+    if (tm) CK(cudaEventRecord(tm->ev[1], c->stream));
+    k_step_mid<T, C, EXACT><<<mid_blocks, 256, 0, c->stream>>>(p, pr);
+    if (tm) CK(cudaEventRecord(tm->ev[2], c->stream));
+    k_step_e<T, C, EXACT><<<grd, blk, 0, c->stream>>>(p);
+    if (tm) CK(cudaEventRecord(tm->ev[3], c->stream));
+    if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, c->stream>>>(p.f, p.g, ff, pr, c->d_ts);
+    if (tm) {
+      CK(cudaEventRecord(tm->ev[4], c->stream));
+      CK(cudaEventSynchronize(tm->ev[4]));
+      for (int q = 0; q < 4; q++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, tm->ev[q], tm->ev[q + 1]));
+        tm->ms[q] += ms;
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+template <typename T>
+ArrayCoef<T> array_coef(const fdtd_ctx* c) {
+  ArrayCoef<T> a{};
+  for (int comp = 0; comp < 6; comp++)
+    for (int w = 0; w < 3; w++) {
+      const int id = comp < 3 ? 9 + 3 * comp + w : 3 * (comp - 3) + w;
+      a.c[comp][w] = (const T*)c->coef[id];
+    }
+  return a;
+}
+
+// Material tables and 1/kappa profiles to the device (once per change; never
+// called while the stream is being captured).
+int prepare_table(fdtd_ctx* c, TableCoef* out) {
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  if (!c->d_tab) {
+    int rc = dalloc(c, (void**)&c->d_tab, 6 * kTableRows * 3 * sizeof(float));
+    if (rc) return rc;
+    for (int q = 0; q < 6; q++) {
+      rc = dalloc(c, (void**)&c->d_invk[q], (n_axis[q % 3] + 1) * sizeof(float));
+      if (rc) return rc;
+    }
+  }
+  if (c->table_dirty) {
+    std::vector<float> tab(6 * kTableRows * 3, 0.f);
+    for (int f = 0; f < 6; f++) {
+      const std::vector<float>& t = c->table[(f + 3) % 6];
+      std::copy(t.begin(), t.end(), tab.begin() + f * kTableRows * 3);
+    }
+    CK(cudaMemcpy(c->d_tab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; a++) {
+      std::vector<float> ie(n_axis[a] + 1, 1.f), im(n_axis[a] + 1, 1.f);
+      for (int side = 0; side < 2; side++) {
+        const HostFace& h = c->face[2 * a + side];
+        if (!h.present) continue;
+        std::vector<float> ke(h.nc), km(h.nc);
+        CK(cudaMemcpy(ke.data(), h.inv_k[0], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(km.data(), h.inv_k[1], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int q = 0; q < h.nc; q++) {
+          ie[h.e_start + q] = ke[q];
+          im[h.m_start + q] = km[q];
+        }
+      }
+      CK(cudaMemcpy(c->d_invk[a], ie.data(), ie.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->d_invk[3 + a], im.data(), im.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  }
+  TableCoef t{};
+  for (int f = 0; f < 6; f++) t.ids[f] = c->ids[(f + 3) % 6];
+  t.tab = c->d_tab;
+  for (int q = 0; q < 6; q++) t.invk[q] = c->d_invk[q];
+  t.d[0] = (float)c->dx;
+  t.d[1] = (float)c->dy;
+  t.d[2] = (float)c->dz;
+  *out = t;
+  c->table_dirty = false;
+  return FDTD_OK;
+}
+
+int enqueue(fdtd_ctx* c, int count, KernelTimer* tm = nullptr) {
+  if (c->prec == FDTD_PREC_F64) return enqueue_steps<double, ArrayCoef<double>, true>(c, array_coef<double>(c), count, tm);
+  if (c->prec == FDTD_PREC_F32) return enqueue_steps<float, ArrayCoef<float>, true>(c, array_coef<float>(c), count, tm);
+  return enqueue_steps<float, TableCoef, false>(c, c->tcoef, count, tm);
+}
+
+constexpr int kGraphSteps = 64;
+
+int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* tm = nullptr) {
+  if (count < 0) return fail(FDTD_ERR_BADARG, "negative step count %d", count);
+  if (c->ts + count > c->nsteps)
+    return fail(FDTD_ERR_BADARG, "running %d steps from step %d exceeds numberOfTimeSteps=%d", count, c->ts,
+                c->nsteps);
+  int rc = check_ready(c);
+  if (rc) return rc;
+  rc = ensure_traces(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  if (c->prec == FDTD_PREC_F32_TABLE && c->table_dirty) {
+    rc = prepare_table(c, &c->tcoef);
+    if (rc) return rc;
+  }
+  int left = count;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (elapsed_ms) {
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, c->stream));
+  }
+  if (tm) {
+    rc = enqueue(c, left, tm);
+    if (rc) return rc;
+    left = 0;
+  }
+  // whole batches through a cached graph of kGraphSteps steps
+  while (left >= kGraphSteps) {
+    if (!c->graph || c->dirty) {
+      if (c->graph) cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int erc = enqueue(c, kGraphSteps);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+      if (erc) return erc;
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&c->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      c->graph_steps = kGraphSteps;
+      c->dirty = false;
+    }
+    CK(cudaGraphLaunch(c->graph, c->stream));
+    left -= kGraphSteps;
+  }
+  if (left > 0) {
+    rc = enqueue(c, left);
+    if (rc) return rc;
+  }
+  if (elapsed_ms) {
+    CK(cudaEventRecord(ev1, c->stream));
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->ts += count;
+  int st[2];
+  CK(cudaMemcpy(st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st[0] != 0) return fail(FDTD_ERR_NONFINITE, "non-finite port sample at step %d", st[1]);
+  return FDTD_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Handle API
+// ===========================================================================
+extern "C" {
+
+static int set_rows(fdtd_ctx* c, int comp, const std::vector<double>& rows);
+
+const char* fdtd_last_error(void) { return g_err; }
+
+int fdtd_device_count(int* count) {
+  if (!count) return fail(FDTD_ERR_BADARG, "count is NULL");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+  *count = n;
+  return FDTD_OK;
+}
+
+int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
+  if (!cfg || !out) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *out = nullptr;
+  if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 2) return fail(FDTD_ERR_BADARG, "grid %dx%dx%d too small", cfg->nx, cfg->ny, cfg->nz);
+  if ((long long)(cfg->nx + 1) * (cfg->ny + 1) * (cfg->nz + 1) > (1LL << 31) - 1)
+    return fail(FDTD_ERR_BADARG, "grid too large for 32-bit component indices");
+  if (cfg->numberOfTimeSteps < 1) return fail(FDTD_ERR_BADARG, "numberOfTimeSteps must be >= 1");
+  if (cfg->precision < FDTD_PREC_F64 || cfg->precision > FDTD_PREC_F32_TABLE)
+    return fail(FDTD_ERR_BADARG, "unknown precision %d", cfg->precision);
+  if (!(cfg->dx > 0 && cfg->dy > 0 && cfg->dz > 0 && cfg->dt > 0)) return fail(FDTD_ERR_BADARG, "non-positive spacing");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev)
+    return fail(FDTD_ERR_CUDA, "CUDA device %d not available", cfg->device);
+  fdtd_ctx* c = new fdtd_ctx();
+  c->device = cfg->device;
+  c->prec = cfg->precision;
+  c->esz = (c->prec == FDTD_PREC_F64) ? 8 : 4;
+  c->nx = cfg->nx; c->ny = cfg->ny; c->nz = cfg->nz;
+  c->dx = cfg->dx; c->dy = cfg->dy; c->dz = cfg->dz; c->dt = cfg->dt;
+  c->nsteps = cfg->numberOfTimeSteps;
+  const long long nx = c->nx, ny = c->ny, nz = c->nz;
+  c->ncomp[0] = (nx + 1) * ny * nz;
+  c->ncomp[1] = nx * (ny + 1) * nz;
+  c->ncomp[2] = nx * ny * (nz + 1);
+  c->ncomp[3] = nx * (ny + 1) * (nz + 1);
+  c->ncomp[4] = (nx + 1) * ny * (nz + 1);
+  c->ncomp[5] = (nx + 1) * (ny + 1) * nz;
+  int rc = FDTD_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(FDTD_ERR_CUDA, "cannot create a stream on device %d", cfg->device);
+  }
+  long long tot = 0;
+  for (int q = 0; q < 6; q++) tot += c->ncomp[q];
+  tot += (ny + 1) * (nz + 1) + 64;  // slack plane past Ez
+  if (!rc) rc = dalloc(c, &c->fields, tot * c->esz);
+  if (!rc) rc = dalloc(c, &c->ex0b, (size_t)(ny + 1) * (nz + 1) * c->esz);
+  if (!rc) rc = dalloc(c, (void**)&c->d_ts, sizeof(int));
+  if (!rc) rc = dalloc(c, (void**)&c->d_status, 2 * sizeof(int));
+  if (!rc) {
+    int init_ts = -1;
+    int st[2] = {0, 1 << 30};
+    if (cudaMemcpy(c->d_ts, &init_ts, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_status, st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = fail(FDTD_ERR_CUDA, "cannot initialise step counter");
+  }
+  if (!rc && c->prec != FDTD_PREC_F32_TABLE) {
+    for (int q = 0; q < 18 && !rc; q++) rc = dalloc(c, &c->coef[q], coef_count(c, q) * c->esz);
+  }
+  if (!rc && c->prec == FDTD_PREC_F32_TABLE) {
+    for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6]);
+  }
+  if (!rc) rc = ensure_traces(c);
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "stream sync failed");
+  if (rc) {
+    std::string msg = g_err;
+    fdtd_free(c);
+    return fail(rc, "%s", msg.c_str());
+  }
+  *out = c;
+  return FDTD_OK;
+}
+
+void fdtd_free(fdtd_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (void* p : c->owned) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int fdtd_ctx_upload_coeff(fdtd_ctx* c, int which, const double* host, long n) {
+  if (!c || !host) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->prec == FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "material-table problem takes fdtd_ctx_upload_material");
+  if (which < 0 || which >= 18) return fail(FDTD_ERR_BADARG, "coefficient id %d out of range 0..17", which);
+  if (n != coef_count(c, which)) return fail(FDTD_ERR_BADARG, "coefficient %d: got %ld values, expected %lld", which, n, coef_count(c, which));
+  CK(cudaSetDevice(c->device));
+  int rc = upload_real(c, c->coef[which], host, n);
+  if (!rc) c->coef_set[which] = true;
+  return rc;
+}
+
+int fdtd_ctx_upload_cpml(fdtd_ctx* c, int f, int nc, const double* b_e, const double* a_e, const double* b_m,
+                         const double* a_m, const double* kappa_e, const double* kappa_m, const double* CPsi0,
+                         long n0, const double* CPsi1, long n1, const double* CPsi2, long n2, const double* CPsi3,
+                         long n3, int m_start, int e_start) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (f < 0 || f >= 6) return fail(FDTD_ERR_BADARG, "face id %d out of range 0..5", f);
+  if (nc < 0) return fail(FDTD_ERR_BADARG, "negative cell count");
+  const int axis_n = f / 2 == 0 ? c->nx : (f / 2 == 1 ? c->ny : c->nz);
+  if (nc > axis_n / 2) return fail(FDTD_ERR_BADARG, "face %d: %d CPML cells do not fit in %d cells", f, nc, axis_n);
+  if (m_start < 0 || m_start + nc > axis_n) return fail(FDTD_ERR_BADARG, "face %d: H band [%d,%d) outside [0,%d)", f, m_start, m_start + nc, axis_n);
+  if (e_start < 1 || e_start + nc > axis_n) return fail(FDTD_ERR_BADARG, "face %d: E band [%d,%d) outside [1,%d)", f, e_start, e_start + nc, axis_n);
+  if (nc > 0 && (!b_e || !a_e || !b_m || !a_m)) return fail(FDTD_ERR_BADARG, "face %d: missing b/a profile", f);
+  const bool table = c->prec == FDTD_PREC_F32_TABLE;
+  if (table && nc > 0 && (!kappa_e || !kappa_m)) return fail(FDTD_ERR_BADARG, "face %d: material-table problems need kappa profiles", f);
+  long long want[4];
+  psi_sizes(c, f, nc, want);
+  const double* cp[4] = {CPsi0, CPsi1, CPsi2, CPsi3};
+  const long got[4] = {n0, n1, n2, n3};
+  for (int s = 0; s < 4; s++) {
+    if (table) continue;  // CPsi comes from the coefficient tables
+    if (got[s] != want[s] || (want[s] > 0 && !cp[s]))
+      return fail(FDTD_ERR_BADARG, "face %d slot %d: got %ld CPsi values, expected %lld", f, s, got[s], want[s]);
+  }
+  CK(cudaSetDevice(c->device));
+  HostFace& h = c->face[f];
+  for (int s = 0; s < 4; s++) { dfree(c, h.prof[s]); dfree(c, h.psi[s]); dfree(c, h.cpsi[s]); }
+  dfree(c, h.inv_k[0]); dfree(c, h.inv_k[1]);
+  h = HostFace();
+  h.present = nc > 0;
+  h.nc = nc; h.m_start = m_start; h.e_start = e_start;
+  invalidate(c);
+  if (nc == 0) return FDTD_OK;
+  const double* pr[4] = {b_e, a_e, b_m, a_m};
+  int rc = FDTD_OK;
+  for (int s = 0; s < 4 && !rc; s++) {
+    rc = dalloc(c, &h.prof[s], nc * c->esz);
+    if (!rc) rc = upload_real(c, h.prof[s], pr[s], nc);
+  }
+  for (int s = 0; s < 4 && !rc; s++) {
+    h.n[s] = want[s];
+    rc = dalloc(c, &h.psi[s], want[s] * c->esz);
+    if (!rc && !table) {
+      rc = dalloc(c, &h.cpsi[s], want[s] * c->esz);
+      if (!rc) rc = upload_real(c, h.cpsi[s], cp[s], want[s]);
+    }
+  }
+  if (!rc && table) {
+    std::vector<float> ik(nc);
+    const double* kp[2] = {kappa_e, kappa_m};
+    for (int s = 0; s < 2 && !rc; s++) {
+      for (int q = 0; q < nc; q++) {
+        if (!(kp[s][q] > 0)) return fail(FDTD_ERR_BADARG, "face %d: kappa must be positive", f);
+        ik[q] = (float)(1.0 / kp[s][q]);
+      }
+      rc = dalloc(c, (void**)&h.inv_k[s], nc * sizeof(float));
+      if (!rc && cudaMemcpy(h.inv_k[s], ik.data(), nc * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(FDTD_ERR_CUDA, "kappa upload failed");
+    }
+  }
+  if (rc) h.present = false;
+  return rc;
+}
+
+int fdtd_ctx_add_vsource(fdtd_ctx* c, int dir, const int* idx, const double* coef, int count, const double* wave,
+                         int nSteps) {
+  if (!c || !idx || !coef || !wave) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (dir < 0 || dir > 2) return fail(FDTD_ERR_BADARG, "source direction %d not in 0..2", dir);
+  if (count <= 0) return fail(FDTD_ERR_BADARG, "source has no cells");
+  if (nSteps < c->nsteps) return fail(FDTD_ERR_BADARG, "waveform has %d values, need %d", nSteps, c->nsteps);
+  if ((int)c->src.size() >= kMaxSources) return fail(FDTD_ERR_BADARG, "at most %d sources", kMaxSources);
+  // component extents of E_dir
+  const int ni = dir == 0 ? c->nx : c->nx + 1, nj = dir == 1 ? c->ny : c->ny + 1, nk = dir == 2 ? c->nz : c->nz + 1;
+  const long long n = (long long)ni * nj * nk;
+  int bi0 = 1 << 30, bi1 = -1, bj0 = 1 << 30, bj1 = -1, bk0 = 1 << 30, bk1 = -1;
+  for (int q = 0; q < count; q++) {
+    if (idx[q] < 0 || idx[q] >= n) return fail(FDTD_ERR_BADARG, "source index %d out of range", idx[q]);
+    const int i = idx[q] / (nj * nk), j = (idx[q] / nk) % nj, k = idx[q] % nk;
+    bi0 = std::min(bi0, i); bi1 = std::max(bi1, i);
+    bj0 = std::min(bj0, j); bj1 = std::max(bj1, j);
+    bk0 = std::min(bk0, k); bk1 = std::max(bk1, k);
+  }
+  // the list must be the box in createLinearIndexList order (grid.js:228-243)
+  const long long bn = (long long)(bi1 - bi0 + 1) * (bj1 - bj0 + 1) * (bk1 - bk0 + 1);
+  if (bn != count) return fail(FDTD_ERR_BADARG, "source cells do not form a box");
+  int q = 0;
+  for (int k = bk0; k <= bk1; k++)
+    for (int j = bj0; j <= bj1; j++)
+      for (int i = bi0; i <= bi1; i++, q++)
+        if (idx[q] != (i * nj + j) * nk + k) return fail(FDTD_ERR_BADARG, "source cells not in k-j-i box order");
+  for (int q2 = 0; q2 < count; q2++)
+    if (!std::isfinite(coef[q2])) return fail(FDTD_ERR_BADARG, "non-finite source coefficient");
+  CK(cudaSetDevice(c->device));
+  HostSource s;
+  s.box = SourceBox{dir, bi0, bi1, bj0, bj1, bk0, bk1};
+  s.count = count;
+  int rc = dalloc(c, &s.cs, count * c->esz);
+  if (!rc) rc = upload_real(c, s.cs, coef, count);
+  if (!rc) rc = dalloc(c, &s.wave, (size_t)c->nsteps * c->esz);
+  if (!rc) rc = upload_real(c, s.wave, wave, c->nsteps);
+  if (rc) return rc;
+  c->src.push_back(s);
+  invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_add_svoltage(fdtd_ctx* c, int dir, const int* idx, int count, double Csvf) {
+  if (!c || !idx) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (dir < 0 || dir > 2) return fail(FDTD_ERR_BADARG, "probe direction %d not in 0..2", dir);
+  if (count <= 0) return fail(FDTD_ERR_BADARG, "probe has no cells");
+  if ((int)c->vprobe.size() >= kMaxProbes) return fail(FDTD_ERR_BADARG, "at most %d voltage probes", kMaxProbes);
+  const long long n = c->ncomp[3 + dir];
+  for (int q = 0; q < count; q++)
+    if (idx[q] < 0 || idx[q] >= n) return fail(FDTD_ERR_BADARG, "probe index %d out of range", idx[q]);
+  CK(cudaSetDevice(c->device));
+  HostVProbe p{dir, count, nullptr, Csvf};
+  int rc = dalloc(c, (void**)&p.idx, count * sizeof(int));
+  if (rc) return rc;
+  CK(cudaMemcpy(p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
+  c->vprobe.push_back(p);
+  invalidate(c);
+  return ensure_traces(c);
+}
+
+int fdtd_ctx_add_scurrent(fdtd_ctx* c, const int* comp, const int* idx, const double* w, int count) {
+  if (!c || !comp || !idx || !w) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (count <= 0) return fail(FDTD_ERR_BADARG, "probe has no samples");
+  if ((int)c->iprobe.size() >= kMaxProbes) return fail(FDTD_ERR_BADARG, "at most %d current probes", kMaxProbes);
+  for (int q = 0; q < count; q++) {
+    if (comp[q] < 0 || comp[q] > 2) return fail(FDTD_ERR_BADARG, "current probe component %d not in 0..2", comp[q]);
+    if (idx[q] < 0 || idx[q] >= c->ncomp[comp[q]]) return fail(FDTD_ERR_BADARG, "current probe index %d out of range", idx[q]);
+  }
+  CK(cudaSetDevice(c->device));
+  HostIProbe p{count, nullptr, nullptr, nullptr};
+  int rc = dalloc(c, (void**)&p.comp, count * sizeof(int));
+  if (!rc) rc = dalloc(c, (void**)&p.idx, count * sizeof(int));
+  if (!rc) rc = dalloc(c, (void**)&p.w, count * sizeof(double));
+  if (rc) return rc;
+  CK(cudaMemcpy(p.comp, comp, count * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(p.w, w, count * sizeof(double), cudaMemcpyHostToDevice));
+  c->iprobe.push_back(p);
+  invalidate(c);
+  return ensure_traces(c);
+}
+
+int fdtd_ctx_setup_farfield(fdtd_ctx* c, int nFreq, const double* freqs, int li, int lj, int lk, int ui, int uj,
+                            int uk) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (nFreq < 0 || (nFreq > 0 && !freqs)) return fail(FDTD_ERR_BADARG, "bad frequency list");
+  if (c->nFreq > 0) return fail(FDTD_ERR_STATE, "far field already set up");
+  if (nFreq == 0) return FDTD_OK;
+  // the 4-point averages reach one cell outside the box on each side
+  if (li < 2 || lj < 2 || lk < 2 || ui > c->nx || uj > c->ny || uk > c->nz || ui <= li || uj <= lj || uk <= lk)
+    return fail(FDTD_ERR_BADARG, "Huygens box [%d,%d]x[%d,%d]x[%d,%d] does not fit the grid", li, ui, lj, uj, lk, uk);
+  CK(cudaSetDevice(c->device));
+  c->nFreq = nFreq;
+  c->li = li; c->lj = lj; c->lk = lk; c->ui = ui; c->uj = uj; c->uk = uk;
+  const long long ni = ui - li, nj = uj - lj, nk = uk - lk;
+  c->ffsz[0] = nj * nk;
+  c->ffsz[1] = ni * nk;
+  c->ffsz[2] = ni * nj;
+  long long off = 0;
+  for (int a = 0; a < 24; a++) {
+    c->ffoff[a] = off;
+    off += 2 * nFreq * c->ffsz[(a % 12) / 4];
+  }
+  int rc = dalloc(c, (void**)&c->acc, off * sizeof(double));
+  if (rc) return rc;
+  // phasors, evaluated as farfield.js:101-110 does
+  std::vector<double> ph((size_t)c->nsteps * nFreq * 4);
+  for (int ts = 0; ts < c->nsteps; ts++)
+    for (int m = 0; m < nFreq; m++) {
+      const double w = 2 * M_PI * freqs[m];
+      const double wdt = w * c->dt;
+      const double phh = wdt * (ts + 0.5), phe = wdt * (ts + 1);
+      double* q = &ph[((size_t)ts * nFreq + m) * 4];
+      q[0] = std::cos(phh);
+      q[1] = -std::sin(phh);
+      q[2] = std::cos(phe);
+      q[3] = -std::sin(phe);
+    }
+  rc = dalloc(c, (void**)&c->ph, ph.size() * sizeof(double));
+  if (rc) return rc;
+  CK(cudaMemcpy(c->ph, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice));
+  invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_upload_material(fdtd_ctx* c, int comp, const unsigned char* ids, long n, const double* table, int rows) {
+  if (!c || !ids || !table) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table problem");
+  if (comp < 0 || comp > 5) return fail(FDTD_ERR_BADARG, "component %d not in 0..5", comp);
+  const long long want = c->ncomp[(comp + 3) % 6];
+  if (n != want) return fail(FDTD_ERR_BADARG, "component %d: got %ld ids, expected %lld", comp, n, want);
+  if (rows < 1 || rows > kTableRows) return fail(FDTD_ERR_BADARG, "table rows %d not in 1..%d", rows, kTableRows);
+  for (long q = 0; q < n; q++)
+    if (ids[q] >= rows) return fail(FDTD_ERR_BADARG, "material id %d >= table rows %d", ids[q], rows);
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpy(c->ids[comp], ids, n, cudaMemcpyHostToDevice));
+  int rc = set_rows(c, comp, std::vector<double>(table, table + 3 * rows));
+  if (rc) return rc;
+  c->ids_set[comp] = true;
+  invalidate(c);
+  return FDTD_OK;
+}
+
+// Coefficient triple (self, curl1, curl2) of a component for an averaged
+// material pair, as coefficients.js:22-116 evaluates it (no kappa).
+static void coef_row(const fdtd_ctx* c, int comp, double e, double s, double out[3]) {
+  const double dt = c->dt;
+  const double tdx = 2 * dt / c->dx, tdy = 2 * dt / c->dy, tdz = 2 * dt / c->dz;
+  const double scale = comp < 3 ? 8.854187817e-12 : 4 * M_PI * 1e-7;
+  const double a = 2 * e * scale;
+  const double b = dt * s;
+  const double denom = a + b;
+  // curl numerators (coefficients.js:32-106): Ex tdy,-tdz | Ey tdz,-tdx | Ez tdx,-tdy |
+  // Hx tdz,-tdy | Hy tdx,-tdz | Hz tdy,-tdx
+  static const int sel1[6] = {1, 2, 0, 2, 0, 1}, sel2[6] = {2, 0, 1, 1, 2, 0};
+  const double t[3] = {tdx, tdy, tdz};
+  const double n1 = t[sel1[comp]];
+  const double n2 = -t[sel2[comp]];
+  out[0] = (a - b) / denom;
+  out[1] = n1 / denom;
+  out[2] = n2 / denom;
+}
+
+static int set_rows(fdtd_ctx* c, int comp, const std::vector<double>& rows) {
+  const int nrows = (int)rows.size() / 3;
+  if (nrows > kTableRows) return fail(FDTD_ERR_BADARG, "component %d needs %d coefficient rows (limit %d)", comp, nrows, kTableRows);
+  c->rows64[comp] = rows;
+  c->table[comp].assign(3 * kTableRows, 0.f);
+  for (size_t r = 0; r < rows.size(); r++) c->table[comp][r] = (float)rows[r];
+  return FDTD_OK;
+}
+
+int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, int ntypes, const double* props,
+                            int nplates, const int* plates, const double* plate_sigma) {
+  if (!c || !mat || !props || (nplates > 0 && (!plates || !plate_sigma))) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table problem");
+  if (ncells != (long)c->nx * c->ny * c->nz) return fail(FDTD_ERR_BADARG, "material grid of %ld cells, need %lld", ncells, (long long)c->nx * c->ny * c->nz);
+  if (ntypes < 1 || ntypes > 48) return fail(FDTD_ERR_BADARG, "%d material slots (1..48 supported)", ntypes);
+  if (nplates < 0 || nplates > kMaxPlates) return fail(FDTD_ERR_BADARG, "%d plates (at most %d)", nplates, kMaxPlates);
+  unsigned char mmax = 0;
+  for (long q = 0; q < ncells; q++) mmax = std::max(mmax, mat[q]);
+  if (mmax >= ntypes) return fail(FDTD_ERR_BADARG, "material id %d has no properties", mmax);
+  MatBuild b{};
+  b.nx = c->nx; b.ny = c->ny; b.nz = c->nz; b.M = ntypes; b.nplates = nplates;
+  std::vector<double> psig;  // distinct plate conductivities
+  const int ext[3][3] = {{c->nx, c->ny + 1, c->nz + 1}, {c->nx + 1, c->ny, c->nz + 1}, {c->nx + 1, c->ny + 1, c->nz}};
+  for (int q = 0; q < nplates; q++) {
+    const int* P = plates + 7 * q;
+    if (P[0] < 0 || P[0] > 2) return fail(FDTD_ERR_BADARG, "plate %d: component %d not in 0..2", q, P[0]);
+    const int* e = ext[P[0]];
+    if (P[1] < 0 || P[2] >= e[0] || P[3] < 0 || P[4] >= e[1] || P[5] < 0 || P[6] >= e[2] || P[1] > P[2] || P[3] > P[4] || P[5] > P[6])
+      return fail(FDTD_ERR_BADARG, "plate %d: box outside its component array", q);
+    int sid = -1;
+    for (size_t u = 0; u < psig.size(); u++)
+      if (psig[u] == plate_sigma[q]) sid = (int)u;
+    if (sid < 0) { sid = (int)psig.size(); psig.push_back(plate_sigma[q]); }
+    b.plate[q] = PlateBox{P[0], P[1], P[2], P[3], P[4], P[5], P[6], sid};
+  }
+  CK(cudaSetDevice(c->device));
+  unsigned char* d_mat = nullptr;
+  uint8_t *d_present = nullptr, *d_map = nullptr;
+  const long long M = ntypes;
+  const long long ncode_e = (M * M * M * M + 1) * (long long)(psig.size() + 1);
+  const long long ncode_h = M * M + 1;
+  int rc = FDTD_OK;
+  if (cudaMalloc(&d_mat, ncells) != cudaSuccess || cudaMalloc(&d_present, std::max(ncode_e, ncode_h)) != cudaSuccess ||
+      cudaMalloc(&d_map, std::max(ncode_e, ncode_h)) != cudaSuccess) {
+    rc = fail(FDTD_ERR_OOM, "material build buffers");
+  }
+  if (!rc && cudaMemcpy(d_mat, mat, ncells, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "material grid upload");
+  b.mat = d_mat;
+  const double* t_eps = props;  // props rows: eps_r, mu_r, sigma_e, sigma_m per type id
+  std::vector<uint8_t> present, map;
+  for (int comp = 0; comp < 6 && !rc; comp++) {
+    const long long ncode = comp < 3 ? ncode_e : ncode_h;
+    present.assign(ncode, 0);
+    if (cudaMemset(d_present, 0, ncode) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "memset"); break; }
+    k_material_mark<<<148 * 8, 256, 0, c->stream>>>(b, comp, d_present);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+        cudaMemcpy(present.data(), d_present, ncode, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      rc = fail(FDTD_ERR_CUDA, "material mark: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    std::map<std::pair<double, double>, int> rowof;
+    std::vector<double> rows;
+    map.assign(ncode, 0);
+    const long long fill = comp < 3 ? M * M * M * M : M * M;
+    for (long long code = 0; code < ncode; code++) {
+      if (!present[code]) continue;
+      double e, s;
+      if (comp < 3) {
+        const long long base = code % (fill + 1), sid = code / (fill + 1) - 1;
+        if (base == fill) {
+          e = 1.0; s = 0.0;
+        } else {
+          const long long m1 = base % M, m2 = (base / M) % M, m3 = (base / (M * M)) % M, m4 = base / (M * M * M);
+          e = 0.25 * (t_eps[4 * m1] + t_eps[4 * m2] + t_eps[4 * m3] + t_eps[4 * m4]);
+          s = 0.25 * (props[4 * m1 + 2] + props[4 * m2 + 2] + props[4 * m3 + 2] + props[4 * m4 + 2]);
+        }
+        if (sid >= 0) s = psig[sid];
+      } else if (code == fill) {
+        e = 1.0; s = 0.0;
+      } else {
+        const long long m1 = code % M, m2 = code / M;
+        const double mu1 = props[4 * m1 + 1], mu2 = props[4 * m2 + 1];
+        e = 2 * mu1 * mu2 / (mu1 + mu2);
+        const double sm1 = props[4 * m1 + 3], sm2 = props[4 * m2 + 3];
+        s = 2 * sm1 * sm2 / (sm1 + sm2);
+      }
+      auto key = std::make_pair(e, s);
+      auto it = rowof.find(key);
+      int r;
+      if (it == rowof.end()) {
+        r = (int)rows.size() / 3;
+        rowof[key] = r;
+        double tr[3];
+        coef_row(c, comp, e, s, tr);
+        rows.insert(rows.end(), tr, tr + 3);
+      } else {
+        r = it->second;
+      }
+      map[code] = (uint8_t)std::min(r, 255);
+    }
+    rc = set_rows(c, comp, rows);
+    if (rc) break;
+    if (cudaMemcpy(d_map, map.data(), ncode, cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "code map upload"); break; }
+    k_material_ids<<<148 * 8, 256, 0, c->stream>>>(b, comp, d_map, c->ids[comp]);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "material ids: %s", cudaGetErrorString(cudaGetLastError())); break; }
+    c->ids_set[comp] = true;
+  }
+  cudaFree(d_mat);
+  cudaFree(d_present);
+  cudaFree(d_map);
+  invalidate(c);
+  return rc;
+}
+
+int fdtd_ctx_override_material(fdtd_ctx* c, int comp, const int* idx, const double* triples, int count) {
+  if (!c || !idx || !triples) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table problem");
+  if (comp < 0 || comp > 5 || !c->ids_set[comp]) return fail(FDTD_ERR_STATE, "component %d has no material ids yet", comp);
+  const long long n = c->ncomp[(comp + 3) % 6];
+  std::vector<double> rows = c->rows64[comp];
+  CK(cudaSetDevice(c->device));
+  for (int q = 0; q < count; q++) {
+    if (idx[q] < 0 || idx[q] >= n) return fail(FDTD_ERR_BADARG, "cell index %d out of range", idx[q]);
+    int r = -1;
+    for (size_t u = 0; u + 2 < rows.size(); u += 3)
+      if (rows[u] == triples[3 * q] && rows[u + 1] == triples[3 * q + 1] && rows[u + 2] == triples[3 * q + 2]) r = (int)u / 3;
+    if (r < 0) {
+      r = (int)rows.size() / 3;
+      rows.insert(rows.end(), triples + 3 * q, triples + 3 * q + 3);
+    }
+    if (r >= kTableRows) return fail(FDTD_ERR_BADARG, "component %d: coefficient rows exceed %d", comp, kTableRows);
+    const uint8_t id = (uint8_t)r;
+    CK(cudaMemcpy(c->ids[comp] + idx[q], &id, 1, cudaMemcpyHostToDevice));
+  }
+  int rc = set_rows(c, comp, rows);
+  invalidate(c);
+  return rc;
+}
+
+int fdtd_ctx_read_material(fdtd_ctx* c, int comp, unsigned char* ids, long n, double* table, int* rows) {
+  if (!c || !ids || !table || !rows) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->prec != FDTD_PREC_F32_TABLE || comp < 0 || comp > 5 || !c->ids_set[comp]) return fail(FDTD_ERR_STATE, "no material ids for component %d", comp);
+  if (n != c->ncomp[(comp + 3) % 6]) return fail(FDTD_ERR_BADARG, "id buffer of %ld, need %lld", n, c->ncomp[(comp + 3) % 6]);
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpy(ids, c->ids[comp], n, cudaMemcpyDeviceToHost));
+  *rows = (int)c->rows64[comp].size() / 3;
+  std::copy(c->rows64[comp].begin(), c->rows64[comp].end(), table);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_run(fdtd_ctx* c, int count) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  return run_steps(c, count);
+}
+
+int fdtd_ctx_run_timed(fdtd_ctx* c, int count, float* ms) {
+  if (!c || !ms) return fail(FDTD_ERR_BADARG, "NULL argument");
+  return run_steps(c, count, ms);
+}
+
+int fdtd_ctx_profile_kernels(fdtd_ctx* c, int count, double* avg_ms) {
+  if (!c || !avg_ms || count < 1) return fail(FDTD_ERR_BADARG, "bad arguments");
+  KernelTimer tm;
+  CK(cudaSetDevice(c->device));
+  for (int q = 0; q < 5; q++) CK(cudaEventCreate(&tm.ev[q]));
+  int rc = run_steps(c, count, nullptr, &tm);
+  for (int q = 0; q < 5; q++) cudaEventDestroy(tm.ev[q]);
+  if (rc) return rc;
+  for (int q = 0; q < 4; q++) avg_ms[q] = tm.ms[q] / count;
+  return FDTD_OK;
+}
+
+int fdtd_ctx_step(const fdtd_ctx* c) { return c ? c->ts : -1; }
+
+int fdtd_status(fdtd_ctx* c, int* code, int* step) {
+  if (!c || !code || !step) return fail(FDTD_ERR_BADARG, "NULL argument");
+  int st[2];
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpy(st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  *code = st[0];
+  *step = st[0] ? st[1] : -1;
+  return FDTD_OK;
+}
+
+int fdtd_ctx_read_trace(fdtd_ctx* c, int kind, int probe, double* out, int n) {
+  if (!c || !out) return fail(FDTD_ERR_BADARG, "NULL argument");
+  const int np = kind == 0 ? (int)c->vprobe.size() : (int)c->iprobe.size();
+  if (kind < 0 || kind > 1 || probe < 0 || probe >= np) return fail(FDTD_ERR_BADARG, "no probe %d of kind %d", probe, kind);
+  if (n < 0 || n > c->nsteps) return fail(FDTD_ERR_BADARG, "bad length %d", n);
+  CK(cudaSetDevice(c->device));
+  const double* src = (kind == 0 ? c->V : c->I) + (size_t)probe * c->nsteps;
+  CK(cudaMemcpy(out, src, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDTD_OK;
+}
+
+int fdtd_ctx_read_field(fdtd_ctx* c, int which, double* host, long n) {
+  if (!c || !host) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (which < 0 || which > 5) return fail(FDTD_ERR_BADARG, "field id %d not in 0..5", which);
+  if (n != c->ncomp[which]) return fail(FDTD_ERR_BADARG, "field %d: buffer of %ld, need %lld", which, n, c->ncomp[which]);
+  CK(cudaSetDevice(c->device));
+  return read_real(c, field_ptr(c, which), host, n);
+}
+
+int fdtd_ctx_read_psi(fdtd_ctx* c, int f, int slot, double* host, long n) {
+  if (!c || !host) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (f < 0 || f > 5 || slot < 0 || slot > 3 || !c->face[f].present) return fail(FDTD_ERR_BADARG, "no Psi slot %d on face %d", slot, f);
+  if (n != c->face[f].n[slot]) return fail(FDTD_ERR_BADARG, "Psi buffer of %ld, need %lld", n, c->face[f].n[slot]);
+  CK(cudaSetDevice(c->device));
+  return read_real(c, c->face[f].psi[slot], host, n);
+}
+
+int fdtd_ctx_read_farfield(fdtd_ctx* c, int array, double* re, double* im, long n) {
+  if (!c || !re || !im) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (c->nFreq == 0) return fail(FDTD_ERR_STATE, "no far field set up");
+  if (array < 0 || array > 23) return fail(FDTD_ERR_BADARG, "array %d not in 0..23", array);
+  const long long m = c->nFreq * c->ffsz[(array % 12) / 4];
+  if (n != m) return fail(FDTD_ERR_BADARG, "far-field buffer of %ld, need %lld", n, m);
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpy(re, c->acc + c->ffoff[array], m * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(im, c->acc + c->ffoff[array] + m, m * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDTD_OK;
+}
+
+// Direct time-to-frequency transform (dft.js:17-38); one block per frequency.
+__global__ void __launch_bounds__(256) k_dft(const double* x, int N, double dt, const double* f, double shift,
+                                             double* re, double* im) {
+  __shared__ double sr[256], si[256];
+  const int m = blockIdx.x;
+  const double w = 2 * M_PI * f[m];
+  double r = 0.0, q = 0.0;
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    const double ph = w * ((n + 1) * dt + shift);
+    double s, c;
+    sincos(ph, &s, &c);
+    r += x[n] * c;
+    q -= x[n] * s;
+  }
+  sr[threadIdx.x] = r;
+  si[threadIdx.x] = q;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sr[threadIdx.x] += sr[threadIdx.x + o];
+      si[threadIdx.x] += si[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    re[m] = sr[0] * dt;
+    im[m] = si[0] * dt;
+  }
+}
+
+int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re, double* im) {
+  if (!x || !freqs || !re || !im || N <= 0 || M <= 0) return fail(FDTD_ERR_BADARG, "bad DFT arguments");
+  double *dx_ = nullptr, *df = nullptr, *dr = nullptr;
+  int rc = FDTD_OK;
+  if (cudaMalloc(&dx_, N * sizeof(double)) != cudaSuccess || cudaMalloc(&df, M * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&dr, 2 * M * sizeof(double)) != cudaSuccess) {
+    rc = fail(FDTD_ERR_OOM, "DFT buffers");
+  } else if (cudaMemcpy(dx_, x, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+             cudaMemcpy(df, freqs, M * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    rc = fail(FDTD_ERR_CUDA, "DFT upload");
+  } else {
+    k_dft<<<M, 256>>>(dx_, N, dt, df, shift, dr, dr + M);
+    if (cudaMemcpy(re, dr, M * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(im, dr + M, M * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(FDTD_ERR_CUDA, "DFT: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  cudaFree(dx_);
+  cudaFree(df);
+  cudaFree(dr);
+  return rc;
+}
+
+// ===========================================================================
+// Legacy global-context API (fdtd_cuda.h), FP32 per-cell coefficients.
+// ===========================================================================
+static fdtd_ctx* g_legacy = nullptr;
+
+int fdtd_init(const FdtdDims* d) {
+  if (!d) return fail(FDTD_ERR_BADARG, "NULL dims");
+  fdtd_free(g_legacy);
+  g_legacy = nullptr;
+  FdtdConfig cfg{d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, d->dt, d->numberOfTimeSteps, FDTD_PREC_F32, 0};
+  return fdtd_create(&cfg, &g_legacy);
+}
+
+static std::vector<double> widen(const float* p, long long n) {
+  std::vector<double> v(std::max<long long>(n, 0));
+  for (long long q = 0; q < n; q++) v[q] = p[q];
+  return v;
+}
+
+int fdtd_upload_coeff(int which, const float* host, int n) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  if (!host) return fail(FDTD_ERR_BADARG, "NULL array");
+  auto v = widen(host, n);
+  return fdtd_ctx_upload_coeff(g_legacy, which, v.data(), n);
+}
+
+int fdtd_upload_cpml(int faceId, int nc, const float* b_e, const float* a_e, const float* b_m, const float* a_m,
+                     const float* CPsi0, int n0, const float* CPsi1, int n1, const float* CPsi2, int n2,
+                     const float* CPsi3, int n3, int m_start, int e_start, int ascending) {
+  (void)ascending;  // the band starts carry the same information
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  if (nc > 0 && (!b_e || !a_e || !b_m || !a_m)) return fail(FDTD_ERR_BADARG, "missing b/a profile");
+  auto be = nc > 0 ? widen(b_e, nc) : std::vector<double>(), ae = nc > 0 ? widen(a_e, nc) : std::vector<double>();
+  auto bm = nc > 0 ? widen(b_m, nc) : std::vector<double>(), am = nc > 0 ? widen(a_m, nc) : std::vector<double>();
+  auto c0 = CPsi0 ? widen(CPsi0, n0) : std::vector<double>(), c1 = CPsi1 ? widen(CPsi1, n1) : std::vector<double>();
+  auto c2 = CPsi2 ? widen(CPsi2, n2) : std::vector<double>(), c3 = CPsi3 ? widen(CPsi3, n3) : std::vector<double>();
+  return fdtd_ctx_upload_cpml(g_legacy, faceId, nc, be.data(), ae.data(), bm.data(), am.data(), nullptr, nullptr,
+                              CPsi0 ? c0.data() : nullptr, n0, CPsi1 ? c1.data() : nullptr, n1,
+                              CPsi2 ? c2.data() : nullptr, n2, CPsi3 ? c3.data() : nullptr, n3, m_start, e_start);
+}
+
+int fdtd_upload_vsource(int dir, const int* idx, const float* coef, int count, const float* waveform, int nSteps) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  if (!coef || !waveform) return fail(FDTD_ERR_BADARG, "NULL array");
+  auto cs = widen(coef, count), wv = widen(waveform, nSteps);
+  return fdtd_ctx_add_vsource(g_legacy, dir, idx, cs.data(), count, wv.data(), nSteps);
+}
+
+int fdtd_upload_svoltage(int dir, const int* idx, int count, float Csvf) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  return fdtd_ctx_add_svoltage(g_legacy, dir, idx, count, Csvf);
+}
+
+int fdtd_upload_scurrent(const int* hxIdx, const float* hxW, int hxN, const int* hyIdx, const float* hyW, int hyN,
+                         const int* hzIdx, const float* hzW, int hzN) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  std::vector<int> comp, idx;
+  std::vector<double> w;
+  const int* I[3] = {hxIdx, hyIdx, hzIdx};
+  const float* W[3] = {hxW, hyW, hzW};
+  const int N[3] = {hxN, hyN, hzN};
+  for (int c = 0; c < 3; c++) {
+    if (N[c] > 0 && (!I[c] || !W[c])) return fail(FDTD_ERR_BADARG, "NULL gather list");
+    for (int q = 0; q < N[c]; q++) {
+      comp.push_back(c);
+      idx.push_back(I[c][q]);
+      w.push_back(W[c][q]);
+    }
+  }
+  return fdtd_ctx_add_scurrent(g_legacy, comp.data(), idx.data(), w.data(), (int)comp.size());
+}
+
+int fdtd_run_batch(int tsStart, int count, float* svOut, float* siOut) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  if (tsStart != g_legacy->ts) return fail(FDTD_ERR_BADARG, "batch starts at %d, the problem is at step %d", tsStart, g_legacy->ts);
+  int rc = fdtd_ctx_run(g_legacy, count);
+  if (rc && rc != FDTD_ERR_NONFINITE) return rc;
+  std::vector<double> tmp(g_legacy->nsteps);
+  if (svOut && !g_legacy->vprobe.empty()) {
+    int r2 = fdtd_ctx_read_trace(g_legacy, 0, 0, tmp.data(), tsStart + count);
+    if (r2) return r2;
+    for (int q = 0; q < count; q++) svOut[q] = (float)tmp[tsStart + q];
+  }
+  if (siOut && !g_legacy->iprobe.empty()) {
+    int r2 = fdtd_ctx_read_trace(g_legacy, 1, 0, tmp.data(), tsStart + count);
+    if (r2) return r2;
+    for (int q = 0; q < count; q++) siOut[q] = (float)tmp[tsStart + q];
+  }
+  return rc;
+}
+
+int fdtd_read_field(int which, float* host, int n) {
+  if (!g_legacy) return fail(FDTD_ERR_STATE, "fdtd_init not called");
+  if (!host) return fail(FDTD_ERR_BADARG, "NULL array");
+  std::vector<double> tmp(std::max(n, 0));
+  int rc = fdtd_ctx_read_field(g_legacy, which, tmp.data(), n);
+  if (rc) return rc;
+  for (int q = 0; q < n; q++) host[q] = (float)tmp[q];
+  return FDTD_OK;
+}
+
+void fdtd_destroy(void) {
+  fdtd_free(g_legacy);
+  g_legacy = nullptr;
+}
+
+}  // extern "C"

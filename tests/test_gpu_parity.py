@@ -1,0 +1,217 @@
+"""GPU parity: the sm_100a engine against the FP64 CPU oracle, through the C ABI.
+
+FP64 (the drop-in path): bit-identical fields, CPML Psi, port traces and far-
+field accumulators.  FP32 paths: port voltage within 1e-3 of its peak (the
+reference's own GPU-vs-CPU bar, js_fdtd/test/validate_cuda.js:115-135) and
+far-field accumulators within 1e-3 relative to their largest magnitude.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import load_package, load_scenario
+from scenarios_small import small_scenario
+
+pkg = load_package()
+from special_topics_b200 import _native as N  # noqa: E402
+from special_topics_b200 import postproc  # noqa: E402
+from special_topics_b200.backend import B200Backend, Engine  # noqa: E402
+from special_topics_b200.scenario import FF_NAMES, build_problem_from_scenario  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "ifa-fr4-substrate": lambda: (load_scenario("ifa-fr4-substrate"), 200),
+    "small-xp": lambda: (small_scenario(1, "xp"), 60),
+    "small-yn": lambda: (small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3)), 60),
+    "small-zp": lambda: (small_scenario(3, "zp", ncpml=(5, 4, 3, 3, 4, 5)), 60),
+}
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    scn, steps = CASES[request.param]()
+    o = oracle.Oracle(scn, steps)
+    o.step(steps)
+    return request.param, scn, steps, o
+
+
+def _psi_sizes(p, fid):
+    f = p.cpml[fid]
+    return [c.size for c in f.cpsi]
+
+
+def test_fp64_bit_identical(case):
+    name, scn, steps, o = case
+    p = build_problem_from_scenario(scn, steps)
+    with Engine(p, "f64") as eng:
+        eng.run(steps)
+        assert eng.step == steps
+        for q in range(o.n_sv):
+            assert np.array_equal(eng.voltages()[q], o.get(f"V:{q}")), f"V{q}"
+        for q in range(o.n_si):
+            assert np.array_equal(eng.currents()[q], o.get(f"I:{q}")), f"I{q}"
+        for fld in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"):
+            assert np.array_equal(eng.field(fld), o.get(fld)), fld
+        for fid in range(6):
+            for s, n in enumerate(_psi_sizes(p, fid)):
+                assert np.array_equal(eng.psi(fid, s, n), o.get(f"psi:{fid}:{s}")), (fid, s)
+        ff = eng.farfield()
+        for a in FF_NAMES:
+            assert np.array_equal(ff[a][0], o.get(f"ff:{a}:0")), a
+            assert np.array_equal(ff[a][1], o.get(f"ff:{a}:1")), a
+        assert eng.status() == (0, -1)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f32-table"])
+def test_fp32_paths_within_tolerance(case, precision):
+    name, scn, steps, o = case
+    p = build_problem_from_scenario(scn, steps)
+    with Engine(p, precision) as eng:
+        eng.run(steps)
+        v, vo = eng.voltages()[0], o.get("V:0")
+        peak = np.abs(vo).max()
+        assert np.abs(v - vo).max() <= 1e-3 * peak, np.abs(v - vo).max() / peak
+        i, io = eng.currents()[0], o.get("I:0")
+        assert np.abs(i - io).max() <= 1e-3 * np.abs(io).max()
+        ff = eng.farfield()
+        for a in FF_NAMES:
+            ref = o.get(f"ff:{a}:0") + 1j * o.get(f"ff:{a}:1")
+            got = ff[a][0] + 1j * ff[a][1]
+            scale = max(np.abs(ref).max(), 1e-300)
+            assert np.abs(got - ref).max() <= 2e-3 * scale, (a, np.abs(got - ref).max() / scale)
+
+
+def test_device_dft_matches_oracle_transform():
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(3000)
+    f = np.linspace(1e8, 1e10, 301)
+    dt = 5.77e-13
+    for shift in (0.0, -dt / 2):
+        re, im = postproc.time_to_freq(x, dt, f, shift)
+        ore, oim = oracle.time_to_freq(x, dt, f, shift)
+        scale = np.abs(ore + 1j * oim).max()
+        assert np.abs((re - ore) + 1j * (im - oim)).max() <= 1e-12 * scale
+
+
+def test_golden_s11_and_cuts_through_engine(golden_out):
+    """The whole CLI pipeline (index.js:63-134) with the engine's traces: S11 and
+    the directivity cuts agree with the reference's out.json."""
+    scn = load_scenario("ifa-fr4-substrate")
+    p = build_problem_from_scenario(scn, 200)
+    with Engine(p, "f64") as eng:
+        eng.run(200)
+        V, I = eng.voltages()[0], eng.currents()[0]
+        acc = eng.farfield()
+    vg = np.array(golden_out["voltages"][0]["values"])
+    assert np.abs(V - vg).max() <= 1e-8 * np.abs(vg).max()
+    freqs = postproc.dft_frequencies(p.dft)
+    s = postproc.port_s11(V, I, p.grid.dt, freqs, 50.0)
+    sg = golden_out["sparams"][0]
+    assert np.abs(s["mag_dB"] - np.array(sg["magnitude_dB"])).max() < 1e-6
+    cuts = postproc.farfield_cuts(acc, p.grid, p.farfield)
+    for c, g in zip(cuts, golden_out["farfield"]):
+        assert c["plane"] == g["plane"]
+        assert np.abs(c["dataTheta_dB"] - np.array(g["dataTheta_dB"])).max() < 1e-3
+        assert np.abs(c["dataPhi_dB"] - np.array(g["dataPhi_dB"])).max() < 1e-3
+
+
+def test_backend_contract_snapshots():
+    scn = small_scenario(4, "xp")
+    p = build_problem_from_scenario(scn, 55)
+    b = B200Backend("f64")
+    assert b.is_available()
+    snaps = list(b.run(p, batch_size=20))
+    assert [s["step"] for s in snaps] == [20, 40, 55]
+    assert all(s["total"] == 55 and s["backend"] == "b200" for s in snaps)
+    assert snaps[-1]["voltage"] == b.engine.voltages()[0][54]
+    b.engine.close()
+
+
+def test_watchdog_reports_nonfinite_port_sample():
+    scn = small_scenario(6, "xp")
+    p = build_problem_from_scenario(scn, 30)
+    p.voltage_sources[0].voltage_per_e_field[7] = np.nan
+    with Engine(p, "f64") as eng:
+        with pytest.raises(N.FdtdError) as ei:
+            eng.run(30)
+        assert ei.value.code == N.FDTD_ERR_NONFINITE
+        assert eng.status() == (N.FDTD_ERR_NONFINITE, 7)
+
+
+def test_legacy_global_api_fp32():
+    """The reference's fdtd_cuda.h call sequence (cudaBackend.js:183-289) on the legacy entry points."""
+    scn = small_scenario(7, "xp")
+    steps = 50
+    p = build_problem_from_scenario(scn, steps)
+    o = oracle.Oracle(scn, steps)
+    o.step(steps)
+    L, g = N.lib(), p.grid
+    dims = N.FdtdDims(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.dt, steps)
+    N.check(L.fdtd_init(ctypes.byref(dims)))
+    try:
+        from special_topics_b200.scenario import COEFF_ORDER
+        for w, nm in enumerate(COEFF_ORDER):
+            a = p.coeffs[nm].astype(np.float32)
+            N.check(L.fdtd_upload_coeff(w, N.fptr(a), a.size))
+        for fid, f in enumerate(p.cpml):
+            pr = [x.astype(np.float32) for x in (f.b_e, f.a_e, f.b_m, f.a_m)]
+            cp = [c.astype(np.float32) for c in f.cpsi]
+            N.check(L.fdtd_upload_cpml(fid, f.nc, *[N.fptr(x) for x in pr], N.fptr(cp[0]), cp[0].size,
+                                       N.fptr(cp[1]), cp[1].size, N.fptr(cp[2]), cp[2].size, N.fptr(cp[3]),
+                                       cp[3].size, f.m_start, f.e_start, fid % 2))
+        vs = p.voltage_sources[0]
+        cs, wv = vs.coef.astype(np.float32), vs.voltage_per_e_field.astype(np.float32)
+        N.check(L.fdtd_upload_vsource(vs.axis, N.iptr(vs.field_indices), N.fptr(cs), cs.size, N.fptr(wv), wv.size))
+        sv = p.sampled_voltages[0]
+        N.check(L.fdtd_upload_svoltage(sv.axis, N.iptr(sv.field_indices), sv.field_indices.size, sv.Csvf))
+        si = p.sampled_currents[0]
+        lists = []
+        for c in range(3):
+            m = si.comp == c
+            lists += [np.ascontiguousarray(si.idx[m]), np.ascontiguousarray(si.w[m].astype(np.float32))]
+        N.check(L.fdtd_upload_scurrent(N.iptr(lists[0]), N.fptr(lists[1]), lists[0].size,
+                                       N.iptr(lists[2]), N.fptr(lists[3]), lists[2].size,
+                                       N.iptr(lists[4]), N.fptr(lists[5]), lists[4].size))
+        vout = np.zeros(steps, np.float32)
+        iout = np.zeros(steps, np.float32)
+        for ts in range(0, steps, 25):
+            N.check(L.fdtd_run_batch(ts, 25, N.fptr(vout[ts:]), N.fptr(iout[ts:])))
+        vo = o.get("V:0")
+        assert np.abs(vout - vo).max() <= 1e-3 * np.abs(vo).max()
+        io = o.get("I:0")
+        assert np.abs(iout - io).max() <= 1e-3 * np.abs(io).max()
+        ez = np.zeros(p.grid.shapes["Ez"], np.float32).ravel()
+        N.check(L.fdtd_read_field(5, N.fptr(ez), ez.size))
+        assert np.abs(ez - o.get("Ez")).max() <= 1e-3 * np.abs(o.get("Ez")).max()
+    finally:
+        L.fdtd_destroy()
+
+
+@pytest.mark.parametrize("name", ["small-xp", "small-zp", "ifa-fr4-substrate"])
+def test_device_material_tables_match_host_tables(name):
+    """fdtd_ctx_build_material (GPU) gives every cell the same FP64 coefficient
+    triple as the numpy construction from the reference's per-cell arrays."""
+    scn, steps = CASES[name]()
+    p = build_problem_from_scenario(scn, steps)
+    q = build_problem_from_scenario(scn, steps, per_cell=False)
+    from special_topics_b200.tables import COMPONENTS, build_tables
+    host = build_tables(p)
+    with Engine(q, "f32-table") as eng:
+        for comp in COMPONENTS:
+            ids, tab = eng.material(comp)
+            hids, htab = host[comp]
+            assert np.array_equal(tab[ids], htab[hids]), comp
+
+
+def test_device_tables_run_matches_host_tables_run():
+    scn, steps = CASES["small-yn"]()
+    p = build_problem_from_scenario(scn, steps)
+    q = build_problem_from_scenario(scn, steps, per_cell=False)
+    with Engine(p, "f32-table", host_tables=True) as a, Engine(q, "f32-table") as b:
+        a.run(steps)
+        b.run(steps)
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        assert np.array_equal(a.field("Ez"), b.field("Ez"))
