@@ -200,6 +200,21 @@ int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, lon
 int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,
              double* im);
 
+/* The same transform as fdtd_dft, for callers that must not allocate device
+ * memory: a host whose device memory is owned by another component's pool or
+ * budget, or a loop that cannot afford cudaMalloc/cudaFree, which may
+ * synchronise the whole device.  No counterpart in the reference.
+ * Nothing is allocated or freed: inputs and outputs are staged through one
+ * fixed device array of 45,056 doubles (352 KiB), which every GPU that loads
+ * the library holds until the process exits.  Limits: N <= 32768 samples and
+ * M <= 4096 frequencies; larger calls fail with FDTD_ERR_BADARG.  The first
+ * call on a device looks up that array's address, so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU (from several host threads) race and must be serialised by the
+ * caller.  Each call writes every value it reads, so no call sees another's. */
+int fdtd_dft_noalloc(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,
+                     double* im);
+
 #ifdef __cplusplus
 }
 #endif

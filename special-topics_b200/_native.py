@@ -32,6 +32,7 @@ EXPORTS = (
     "fdtd_ctx_override_material", "fdtd_ctx_read_material", "fdtd_ctx_run", "fdtd_ctx_run_timed",
     "fdtd_ctx_profile_kernels", "fdtd_ctx_step", "fdtd_status",
     "fdtd_ctx_read_trace", "fdtd_ctx_read_field", "fdtd_ctx_read_psi", "fdtd_ctx_read_farfield", "fdtd_dft",
+    "fdtd_dft_noalloc",
 )
 
 
@@ -112,6 +113,7 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_read_psi.argtypes = [v, i, i, dp, lp]
     L.fdtd_ctx_read_farfield.argtypes = [v, i, dp, dp, lp]
     L.fdtd_dft.argtypes = [dp, i, d, dp, i, d, dp, dp]
+    L.fdtd_dft_noalloc.argtypes = [dp, i, d, dp, i, d, dp, dp]
     L.fdtd_init.argtypes = [P(FdtdDims)]
     L.fdtd_upload_coeff.argtypes = [i, fp, i]
     L.fdtd_upload_cpml.argtypes = [i, i, fp, fp, fp, fp, fp, i, fp, i, fp, i, fp, i, i, i, i]

@@ -18,6 +18,7 @@
 #include "fdtd_step.cuh"
 
 #include <map>
+#include <mutex>
 #include <utility>
 
 using namespace fdtd;
@@ -1110,6 +1111,62 @@ int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, doub
   cudaFree(df);
   cudaFree(dr);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of fdtd_dft.  Its device staging area is this
+// file-scope array instead of cudaMalloc'd buffers, so a call allocates and
+// frees nothing.  Every GPU that loads the library holds the array until the
+// process exits.  Layout: samples | frequencies | re | im.
+// ---------------------------------------------------------------------------
+constexpr int kDftNoAllocMaxSamples = 32768;
+constexpr int kDftNoAllocMaxFreqs = 4096;
+static __device__ __align__(256) double g_dft_scratch[kDftNoAllocMaxSamples + 3 * kDftNoAllocMaxFreqs];
+
+// The array's device address, looked up once per device with that device
+// current.  In host code `g_dft_scratch` only names a host-side stand-in, so
+// the kernel must be given this address, never the symbol itself.
+static int dft_scratch_address(double** out) {
+  constexpr int kMaxDevices = 64;
+  static double* addr[kMaxDevices] = {};
+  static std::mutex lock;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(FDTD_ERR_CUDA, "device ordinal %d not supported", dev);
+  std::lock_guard<std::mutex> g(lock);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_dft_scratch);
+    if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "cudaGetSymbolAddress(dft scratch): %s", cudaGetErrorString(e));
+    addr[dev] = (double*)p;
+  }
+  *out = addr[dev];
+  return FDTD_OK;
+}
+
+int fdtd_dft_noalloc(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,
+                     double* im) {
+  if (!x || !freqs || !re || !im) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (N <= 0 || N > kDftNoAllocMaxSamples)
+    return fail(FDTD_ERR_BADARG, "fdtd_dft_noalloc: %d samples, must be 1..%d", N, kDftNoAllocMaxSamples);
+  if (M <= 0 || M > kDftNoAllocMaxFreqs)
+    return fail(FDTD_ERR_BADARG, "fdtd_dft_noalloc: %d frequencies, must be 1..%d", M, kDftNoAllocMaxFreqs);
+  double* s = nullptr;
+  int rc = dft_scratch_address(&s);
+  if (rc) return rc;
+  double* d_x = s;
+  double* d_f = s + kDftNoAllocMaxSamples;
+  double* d_re = d_f + kDftNoAllocMaxFreqs;
+  double* d_im = d_re + kDftNoAllocMaxFreqs;
+  // Every value the kernel reads is written by this call and every output is
+  // fully overwritten, so nothing left by an earlier call needs clearing.
+  CK(cudaMemcpy(d_x, x, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_f, freqs, M * sizeof(double), cudaMemcpyHostToDevice));
+  k_dft<<<M, 256>>>(d_x, N, dt, d_f, shift, d_re, d_im);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(re, d_re, M * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(im, d_im, M * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDTD_OK;
 }
 
 // ===========================================================================
