@@ -177,6 +177,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 side measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--tune-steps", type=int, default=32, help="steps timed per autotuner candidate")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
@@ -250,8 +252,19 @@ def main():
                "note": "one step's share of a whole run through the C ABI: uploads from host buffers, "
                        "K steps, readback of port traces and far-field accumulators"}
 
+    # --- launch shape from the autotuner (timed on a scratch copy of the problem)
+    from special_topics_b200 import autotune
+    tuning = None
+    if not args.no_tune:
+        scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000), 3000,
+                                              per_cell=(args.precision != "f32-table"))
+        tuning = autotune.tune(scratch, args.precision, device=local, steps_per_candidate=args.tune_steps)
+        del scratch
+
     # --- device-timed run
     eng = Engine(prob, args.precision, device=local)
+    if tuning:
+        autotune.set_tiling(eng, tuning["chunk"], tuning["rows"])
     eng.run(W)
     barrier()
     with ClockSampler(local) as clk:
@@ -280,6 +293,7 @@ def main():
                      "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom],
                      "traffic": traffic},
         "kernel_ms": kern,
+        "tiling": {k: tuning[k] for k in ("chunk", "rows", "ms_per_step")} if tuning else "default",
         "clocks": clk.summary(),
         "gpu_launches": 4 * K,
         "e2e": e2e,
@@ -317,8 +331,11 @@ def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
     from special_topics_b200 import workloads
     from special_topics_b200.backend import Engine
     from special_topics_b200.scenario import build_problem_from_scenario
-    p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=K + W + 8), K + W + 8)
+    from special_topics_b200 import autotune
+    p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=1000), 1000)
+    tuning = autotune.tune(p, "f64", steps_per_candidate=16)
     eng = Engine(p, "f64")
+    autotune.set_tiling(eng, tuning["chunk"], tuning["rows"])
     eng.run(W)
     ms = eng.run_timed(K)
     kern = eng.profile_kernels(8)
@@ -328,7 +345,7 @@ def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
     dom = "e" if kern["e"] >= kern["h"] else "h"
     ach = byts[dom] / (kern[dom] / 1e3) / 1e9
     return {"workload": f"scaling-box-{n[0]}x{n[1]}x{n[2]}", "value": p.grid.cells * K / (ms / 1e3) / 1e9,
-            "unit": "Gcell-updates/s", "ms_per_step": ms / K,
+            "unit": "Gcell-updates/s", "ms_per_step": ms / K, "tiling": {"chunk": tuning["chunk"], "rows": tuning["rows"]},
             "roofline": {"kernel": f"k_step_{dom}", "achieved": ach, "peak": peak, "frac": ach / peak}}
 
 

@@ -173,6 +173,12 @@ int fdtd_ctx_read_material(fdtd_ctx* ctx, int comp, unsigned char* ids, long n, 
 /* Runs `count` steps from the handle's current step.  Checks the watchdog at
  * the end and returns FDTD_ERR_NONFINITE if a port sample went non-finite. */
 int fdtd_ctx_run(fdtd_ctx* ctx, int count);
+/* Launch shape of the two step kernels: each thread walks `x_planes_per_thread`
+ * consecutive x planes of one (j, k) column; a block is 32 columns along k by
+ * `block_rows` (1, 2, 4 or 8) along j.  Any shape gives the same results; the
+ * autotuner (special-topics_b200/autotune.py) picks the fastest per grid. */
+int fdtd_ctx_set_tiling(fdtd_ctx* ctx, int x_planes_per_thread, int block_rows);
+int fdtd_ctx_get_tiling(const fdtd_ctx* ctx, int* x_planes_per_thread, int* block_rows);
 /* fdtd_ctx_run that also reports the device time (ms) between CUDA events
  * recorded on the handle's stream before the first and after the last launch. */
 int fdtd_ctx_run_timed(fdtd_ctx* ctx, int count, float* ms);

@@ -1,0 +1,81 @@
+"""Launch-shape autotuner for the step kernels.
+
+Every launch shape computes the same values.  For a problem, the tuner times
+the candidate shapes (x planes per thread x thread rows per block) on a
+scratch copy of the problem, so the caller's engine state is untouched, and
+keeps the fastest.  Results are cached per (precision, nx, ny, nz) in a JSON
+file next to the built library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+
+from . import _native as N
+
+CACHE = os.path.join(N.BUILD_DIR, "tiling_cache.json")
+CHUNKS = (1, 2, 4, 8, 16, 32, 64)
+ROWS = (2, 4, 8)
+
+
+def _key(problem, precision: str) -> str:
+    g = problem.grid
+    return f"{precision}:{g.nx}x{g.ny}x{g.nz}"
+
+
+def _load() -> dict:
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def get_tiling(engine) -> tuple[int, int]:
+    a, b = C.c_int(), C.c_int()
+    N.check(N.lib().fdtd_ctx_get_tiling(engine._h, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def set_tiling(engine, chunk: int, rows: int) -> None:
+    N.check(N.lib().fdtd_ctx_set_tiling(engine._h, int(chunk), int(rows)))
+
+
+def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64, use_cache: bool = True) -> dict:
+    """Returns {"chunk", "rows", "ms_per_step", "table"} for the problem's grid."""
+    from .backend import Engine
+    key = _key(problem, precision)
+    cache = _load()
+    if use_cache and key in cache:
+        return cache[key]
+    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS)) + 8
+    if problem.grid.numberOfTimeSteps < need:
+        raise ValueError(f"the scratch problem needs at least {need} time steps for tuning")
+    nx = problem.grid.nx
+    table = []
+    with Engine(problem, precision, device=device) as eng:
+        eng.run(4)
+        for chunk in CHUNKS:
+            if chunk > nx + 1:
+                continue
+            for rows in ROWS:
+                set_tiling(eng, chunk, rows)
+                eng.run_timed(steps_per_candidate)          # capture and warm the graph
+                ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
+                table.append({"chunk": chunk, "rows": rows, "ms_per_step": ms})
+    best = min(table, key=lambda r: r["ms_per_step"])
+    out = {"chunk": best["chunk"], "rows": best["rows"], "ms_per_step": best["ms_per_step"], "table": table}
+    cache[key] = out
+    os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+    with open(CACHE, "w") as f:
+        json.dump(cache, f, indent=1)
+    return out
+
+
+def apply(engine, precision: str, device: int = 0, scratch_problem=None) -> dict:
+    """Tunes (on scratch_problem, or the engine's own problem rebuilt with enough
+    steps by the caller) and sets the best shape on `engine`."""
+    res = tune(scratch_problem or engine.problem, precision, device)
+    set_tiling(engine, res["chunk"], res["rows"])
+    return res

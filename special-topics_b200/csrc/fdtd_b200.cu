@@ -90,7 +90,7 @@ struct fdtd_ctx {
   bool ids_set[6] = {};
   std::vector<float> table[6];
   std::vector<double> rows64[6];  // the same rows in FP64 (rows x 3), for overrides and readback
-  float* d_tab = nullptr;      // [6][kTableRows][3], field order
+  float* d_tab = nullptr;      // [6][kTableRows] float4 rows (self, curl1, curl2, 0), field order
   float* d_invk[6] = {};       // 1/kappa per axis position: E x y z, H x y z
   bool table_dirty = true;
   TableCoef tcoef{};
@@ -111,6 +111,8 @@ struct fdtd_ctx {
   void* ex0b = nullptr;
   int* d_ts = nullptr;
   int* d_status = nullptr;
+  // launch shape of the step kernels: x planes per thread, thread rows per block
+  int ichunk = 1, block_rows = 8;
   // graph cache
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -141,6 +143,15 @@ void dfree(fdtd_ctx* c, void* p) {
   auto it = std::find(c->owned.begin(), c->owned.end(), p);
   if (it != c->owned.end()) c->owned.erase(it);
   cudaFree(p);
+}
+
+// Copy on the handle's stream and wait.  Every set-up copy goes through here so
+// that it is ordered with the zeroing in dalloc and with the kernels, which all
+// run on that (non-blocking) stream.
+cudaError_t xfer(fdtd_ctx* c, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
 }
 
 // Host FP64 array -> device array of the problem's field type.
@@ -332,6 +343,7 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   p.dcell[0] = (T)c->dx;
   p.dcell[1] = (T)c->dy;
   p.dcell[2] = (T)c->dz;
+  p.ichunk = c->ichunk;
   return p;
 }
 
@@ -348,8 +360,10 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   StepParams<T, C> p = step_params<T, C>(c, coef);
   Probes pr = dev_probes(c);
   FarField ff = dev_ff(c);
-  const dim3 blk(32, 4, 2);
-  const dim3 grd((c->nz + 1 + 31) / 32, (c->ny + 1 + 3) / 4, (c->nx + 1 + 1) / 2);
+  // a thread per (j, k) column walks `ichunk` x planes
+  const dim3 blk(32, c->block_rows);
+  const dim3 grd((c->nz + 1 + 31) / 32, (c->ny + c->block_rows) / c->block_rows,
+                 (c->nx + 1 + c->ichunk - 1) / c->ichunk);
   const long long plane = (long long)c->ny * (c->nz + 1);
   const unsigned mid_blocks = (unsigned)((plane + pr.n_i + 255) / 256);
   const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
@@ -393,7 +407,7 @@ ArrayCoef<T> array_coef(const fdtd_ctx* c) {
 int prepare_table(fdtd_ctx* c, TableCoef* out) {
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   if (!c->d_tab) {
-    int rc = dalloc(c, (void**)&c->d_tab, 6 * kTableRows * 3 * sizeof(float));
+    int rc = dalloc(c, (void**)&c->d_tab, 6 * kTableRows * 4 * sizeof(float));
     if (rc) return rc;
     for (int q = 0; q < 6; q++) {
       rc = dalloc(c, (void**)&c->d_invk[q], (n_axis[q % 3] + 1) * sizeof(float));
@@ -401,36 +415,34 @@ int prepare_table(fdtd_ctx* c, TableCoef* out) {
     }
   }
   if (c->table_dirty) {
-    std::vector<float> tab(6 * kTableRows * 3, 0.f);
+    std::vector<float> tab(6 * kTableRows * 4, 0.f);
     for (int f = 0; f < 6; f++) {
       const std::vector<float>& t = c->table[(f + 3) % 6];
-      std::copy(t.begin(), t.end(), tab.begin() + f * kTableRows * 3);
+      for (int r = 0; r < kTableRows; r++)
+        for (int w = 0; w < 3; w++) tab[(f * kTableRows + r) * 4 + w] = t[3 * r + w];
     }
-    CK(cudaMemcpy(c->d_tab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(xfer(c, c->d_tab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
     for (int a = 0; a < 3; a++) {
       std::vector<float> ie(n_axis[a] + 1, 1.f), im(n_axis[a] + 1, 1.f);
       for (int side = 0; side < 2; side++) {
         const HostFace& h = c->face[2 * a + side];
         if (!h.present) continue;
         std::vector<float> ke(h.nc), km(h.nc);
-        CK(cudaMemcpy(ke.data(), h.inv_k[0], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(km.data(), h.inv_k[1], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(xfer(c, ke.data(), h.inv_k[0], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(xfer(c, km.data(), h.inv_k[1], h.nc * sizeof(float), cudaMemcpyDeviceToHost));
         for (int q = 0; q < h.nc; q++) {
           ie[h.e_start + q] = ke[q];
           im[h.m_start + q] = km[q];
         }
       }
-      CK(cudaMemcpy(c->d_invk[a], ie.data(), ie.size() * sizeof(float), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(c->d_invk[3 + a], im.data(), im.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CK(xfer(c, c->d_invk[a], ie.data(), ie.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CK(xfer(c, c->d_invk[3 + a], im.data(), im.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
   }
   TableCoef t{};
   for (int f = 0; f < 6; f++) t.ids[f] = c->ids[(f + 3) % 6];
-  t.tab = c->d_tab;
-  for (int q = 0; q < 6; q++) t.invk[q] = c->d_invk[q];
-  t.d[0] = (float)c->dx;
-  t.d[1] = (float)c->dy;
-  t.d[2] = (float)c->dz;
+  t.tab = (const float4*)c->d_tab;
+  for (int q = 0; q < 6; q++) t.inv[q] = c->d_invk[q];
   *out = t;
   c->table_dirty = false;
   return FDTD_OK;
@@ -504,7 +516,7 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
   CK(cudaStreamSynchronize(c->stream));
   c->ts += count;
   int st[2];
-  CK(cudaMemcpy(st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  CK(xfer(c, st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
   if (st[0] != 0) return fail(FDTD_ERR_NONFINITE, "non-finite port sample at step %d", st[1]);
   return FDTD_OK;
 }
@@ -570,8 +582,8 @@ int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
   if (!rc) {
     int init_ts = -1;
     int st[2] = {0, 1 << 30};
-    if (cudaMemcpy(c->d_ts, &init_ts, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(c->d_status, st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (xfer(c, c->d_ts, &init_ts, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        xfer(c, c->d_status, st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess)
       rc = fail(FDTD_ERR_CUDA, "cannot initialise step counter");
   }
   if (!rc && c->prec != FDTD_PREC_F32_TABLE) {
@@ -581,6 +593,13 @@ int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
     for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6]);
   }
   if (!rc) rc = ensure_traces(c);
+  if (!rc) {
+    // default launch shape: enough x chunks for about four waves of 2048-thread SMs
+    const long long cols = (long long)(ny + 1) * (nz + 1);
+    const long long want = 4LL * 148 * 2048;
+    long long ch = cols * (nx + 1) / want;
+    c->ichunk = (int)std::max<long long>(1, std::min<long long>(64, ch));
+  }
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "stream sync failed");
   if (rc) {
     std::string msg = g_err;
@@ -667,7 +686,7 @@ int fdtd_ctx_upload_cpml(fdtd_ctx* c, int f, int nc, const double* b_e, const do
         ik[q] = (float)(1.0 / kp[s][q]);
       }
       rc = dalloc(c, (void**)&h.inv_k[s], nc * sizeof(float));
-      if (!rc && cudaMemcpy(h.inv_k[s], ik.data(), nc * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      if (!rc && xfer(c, h.inv_k[s], ik.data(), nc * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
         rc = fail(FDTD_ERR_CUDA, "kappa upload failed");
     }
   }
@@ -729,7 +748,7 @@ int fdtd_ctx_add_svoltage(fdtd_ctx* c, int dir, const int* idx, int count, doubl
   HostVProbe p{dir, count, nullptr, Csvf};
   int rc = dalloc(c, (void**)&p.idx, count * sizeof(int));
   if (rc) return rc;
-  CK(cudaMemcpy(p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
+  CK(xfer(c, p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
   c->vprobe.push_back(p);
   invalidate(c);
   return ensure_traces(c);
@@ -749,9 +768,9 @@ int fdtd_ctx_add_scurrent(fdtd_ctx* c, const int* comp, const int* idx, const do
   if (!rc) rc = dalloc(c, (void**)&p.idx, count * sizeof(int));
   if (!rc) rc = dalloc(c, (void**)&p.w, count * sizeof(double));
   if (rc) return rc;
-  CK(cudaMemcpy(p.comp, comp, count * sizeof(int), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(p.w, w, count * sizeof(double), cudaMemcpyHostToDevice));
+  CK(xfer(c, p.comp, comp, count * sizeof(int), cudaMemcpyHostToDevice));
+  CK(xfer(c, p.idx, idx, count * sizeof(int), cudaMemcpyHostToDevice));
+  CK(xfer(c, p.w, w, count * sizeof(double), cudaMemcpyHostToDevice));
   c->iprobe.push_back(p);
   invalidate(c);
   return ensure_traces(c);
@@ -795,7 +814,7 @@ int fdtd_ctx_setup_farfield(fdtd_ctx* c, int nFreq, const double* freqs, int li,
     }
   rc = dalloc(c, (void**)&c->ph, ph.size() * sizeof(double));
   if (rc) return rc;
-  CK(cudaMemcpy(c->ph, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(xfer(c, c->ph, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice));
   invalidate(c);
   return FDTD_OK;
 }
@@ -810,7 +829,7 @@ int fdtd_ctx_upload_material(fdtd_ctx* c, int comp, const unsigned char* ids, lo
   for (long q = 0; q < n; q++)
     if (ids[q] >= rows) return fail(FDTD_ERR_BADARG, "material id %d >= table rows %d", ids[q], rows);
   CK(cudaSetDevice(c->device));
-  CK(cudaMemcpy(c->ids[comp], ids, n, cudaMemcpyHostToDevice));
+  CK(xfer(c, c->ids[comp], ids, n, cudaMemcpyHostToDevice));
   int rc = set_rows(c, comp, std::vector<double>(table, table + 3 * rows));
   if (rc) return rc;
   c->ids_set[comp] = true;
@@ -884,17 +903,17 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
       cudaMalloc(&d_map, std::max(ncode_e, ncode_h)) != cudaSuccess) {
     rc = fail(FDTD_ERR_OOM, "material build buffers");
   }
-  if (!rc && cudaMemcpy(d_mat, mat, ncells, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "material grid upload");
+  if (!rc && xfer(c, d_mat, mat, ncells, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "material grid upload");
   b.mat = d_mat;
   const double* t_eps = props;  // props rows: eps_r, mu_r, sigma_e, sigma_m per type id
   std::vector<uint8_t> present, map;
   for (int comp = 0; comp < 6 && !rc; comp++) {
     const long long ncode = comp < 3 ? ncode_e : ncode_h;
     present.assign(ncode, 0);
-    if (cudaMemset(d_present, 0, ncode) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "memset"); break; }
+    if (cudaMemsetAsync(d_present, 0, ncode, c->stream) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "memset"); break; }
     k_material_mark<<<148 * 8, 256, 0, c->stream>>>(b, comp, d_present);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
-        cudaMemcpy(present.data(), d_present, ncode, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        xfer(c, present.data(), d_present, ncode, cudaMemcpyDeviceToHost) != cudaSuccess) {
       rc = fail(FDTD_ERR_CUDA, "material mark: %s", cudaGetErrorString(cudaGetLastError()));
       break;
     }
@@ -940,7 +959,7 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
     }
     rc = set_rows(c, comp, rows);
     if (rc) break;
-    if (cudaMemcpy(d_map, map.data(), ncode, cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "code map upload"); break; }
+    if (xfer(c, d_map, map.data(), ncode, cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "code map upload"); break; }
     k_material_ids<<<148 * 8, 256, 0, c->stream>>>(b, comp, d_map, c->ids[comp]);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "material ids: %s", cudaGetErrorString(cudaGetLastError())); break; }
     c->ids_set[comp] = true;
@@ -970,7 +989,7 @@ int fdtd_ctx_override_material(fdtd_ctx* c, int comp, const int* idx, const doub
     }
     if (r >= kTableRows) return fail(FDTD_ERR_BADARG, "component %d: coefficient rows exceed %d", comp, kTableRows);
     const uint8_t id = (uint8_t)r;
-    CK(cudaMemcpy(c->ids[comp] + idx[q], &id, 1, cudaMemcpyHostToDevice));
+    CK(xfer(c, c->ids[comp] + idx[q], &id, 1, cudaMemcpyHostToDevice));
   }
   int rc = set_rows(c, comp, rows);
   invalidate(c);
@@ -982,7 +1001,7 @@ int fdtd_ctx_read_material(fdtd_ctx* c, int comp, unsigned char* ids, long n, do
   if (c->prec != FDTD_PREC_F32_TABLE || comp < 0 || comp > 5 || !c->ids_set[comp]) return fail(FDTD_ERR_STATE, "no material ids for component %d", comp);
   if (n != c->ncomp[(comp + 3) % 6]) return fail(FDTD_ERR_BADARG, "id buffer of %ld, need %lld", n, c->ncomp[(comp + 3) % 6]);
   CK(cudaSetDevice(c->device));
-  CK(cudaMemcpy(ids, c->ids[comp], n, cudaMemcpyDeviceToHost));
+  CK(xfer(c, ids, c->ids[comp], n, cudaMemcpyDeviceToHost));
   *rows = (int)c->rows64[comp].size() / 3;
   std::copy(c->rows64[comp].begin(), c->rows64[comp].end(), table);
   return FDTD_OK;
@@ -991,6 +1010,25 @@ int fdtd_ctx_read_material(fdtd_ctx* c, int comp, unsigned char* ids, long n, do
 int fdtd_ctx_run(fdtd_ctx* c, int count) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
   return run_steps(c, count);
+}
+
+int fdtd_ctx_set_tiling(fdtd_ctx* c, int x_planes_per_thread, int block_rows) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (x_planes_per_thread < 1 || x_planes_per_thread > c->nx + 1)
+    return fail(FDTD_ERR_BADARG, "x planes per thread %d not in 1..%d", x_planes_per_thread, c->nx + 1);
+  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8)
+    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8}", block_rows);
+  c->ichunk = x_planes_per_thread;
+  c->block_rows = block_rows;
+  invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_get_tiling(const fdtd_ctx* c, int* x_planes_per_thread, int* block_rows) {
+  if (!c || !x_planes_per_thread || !block_rows) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *x_planes_per_thread = c->ichunk;
+  *block_rows = c->block_rows;
+  return FDTD_OK;
 }
 
 int fdtd_ctx_run_timed(fdtd_ctx* c, int count, float* ms) {
@@ -1016,7 +1054,7 @@ int fdtd_status(fdtd_ctx* c, int* code, int* step) {
   if (!c || !code || !step) return fail(FDTD_ERR_BADARG, "NULL argument");
   int st[2];
   CK(cudaSetDevice(c->device));
-  CK(cudaMemcpy(st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  CK(xfer(c, st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
   *code = st[0];
   *step = st[0] ? st[1] : -1;
   return FDTD_OK;
@@ -1029,7 +1067,7 @@ int fdtd_ctx_read_trace(fdtd_ctx* c, int kind, int probe, double* out, int n) {
   if (n < 0 || n > c->nsteps) return fail(FDTD_ERR_BADARG, "bad length %d", n);
   CK(cudaSetDevice(c->device));
   const double* src = (kind == 0 ? c->V : c->I) + (size_t)probe * c->nsteps;
-  CK(cudaMemcpy(out, src, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(xfer(c, out, src, n * sizeof(double), cudaMemcpyDeviceToHost));
   return FDTD_OK;
 }
 
@@ -1056,8 +1094,8 @@ int fdtd_ctx_read_farfield(fdtd_ctx* c, int array, double* re, double* im, long 
   const long long m = c->nFreq * c->ffsz[(array % 12) / 4];
   if (n != m) return fail(FDTD_ERR_BADARG, "far-field buffer of %ld, need %lld", n, m);
   CK(cudaSetDevice(c->device));
-  CK(cudaMemcpy(re, c->acc + c->ffoff[array], m * sizeof(double), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(im, c->acc + c->ffoff[array] + m, m * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(xfer(c, re, c->acc + c->ffoff[array], m * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(xfer(c, im, c->acc + c->ffoff[array] + m, m * sizeof(double), cudaMemcpyDeviceToHost));
   return FDTD_OK;
 }
 

@@ -10,19 +10,24 @@
 //               (cpml.js:727-1003) and lumped-source injection (sources.js:271-288)
 //   k_epilogue  (fdtd_common.cuh) port voltages and the running NF-FF DFT
 //
-// The kernels are generic over how a cell finds its update coefficients:
-//   ArrayCoef<T>  the reference's 18 per-cell arrays (FP64 drop-in, FP32 legacy)
-//   TableCoef     one uint8 material id per cell and component into a small
-//                 coefficient table, with the CPML kappa division applied from
-//                 1-D per-axis profiles (FP32 fast path)
-// and over the arithmetic: EXACT uses the _rn intrinsics so that nvcc never
-// fuses a multiply into an add and every cell sees the reference's sequence
-// of rounded FP64 operations; otherwise FMA is allowed.
+// Work split: a thread owns one (j,k) column of the (nx+1, ny+1, nz+1) box and
+// walks a chunk of x planes, updating at every (i,j,k) the components that
+// exist there.  Every field value and Psi element has exactly one writer, the
+// x-neighbour of the previous plane is carried in a register (E(i+1) becomes
+// E(i) for the H update, H(i) becomes H(i-1) for the E update), everything
+// that depends only on (j,k) -- 32-bit offsets, y/z CPML band membership, the
+// y/z 1/kappa factors, source-column hits -- is computed once per thread, and
+// the CPML corrections of a value are applied in registers in the reference's
+// face order xn xp yn yp zn zp right after its bulk update.
 //
-// Each thread owns one (i,j,k) of the (nx+1, ny+1, nz+1) box and updates the
-// components that exist there, so every Psi element and field value has
-// exactly one writer and the CPML corrections of a value are applied in the
-// reference's face order xn xp yn yp zn zp.
+// Generic over how a cell finds its coefficients:
+//   ArrayCoef<T>  the reference's 18 per-cell arrays (FP64 drop-in, FP32 legacy)
+//   TableCoef     one uint8 material id per cell and component into a table of
+//                 (self, curl1, curl2) rows without kappa; 1/kappa comes from 1-D
+//                 per-axis profiles and CPsi = curl coefficient x cell size
+// and over the arithmetic: EXACT uses the _rn intrinsics so nvcc never fuses a
+// multiply into an add and every value sees the reference's sequence of
+// rounded operations; otherwise FMA is allowed.
 #pragma once
 #include "fdtd_common.cuh"
 
@@ -61,48 +66,63 @@ struct Ar<T, false> {
 //   Ex: c1 Cexhz dHz/dy (y faces)  c2 Cexhy dHy/dz (z faces)
 //   Ey: c1 Ceyhx dHx/dz (z faces)  c2 Ceyhz dHz/dx (x faces)
 //   Ez: c1 Cezhy dHy/dx (x faces)  c2 Cezhx dHx/dy (y faces)
+// get(): c0, c1, c2 as used by the update (kappa applied), u1, u2 without kappa.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct ArrayCoef {
+  static constexpr bool kTable = false;
   const T* c[6][3];  // [component][self, curl1, curl2]
-  __device__ __forceinline__ void get(int comp, long long idx, int, int, T& c0, T& c1, T& c2, T& u1,
-                                      T& u2) const {
+  __device__ __forceinline__ void get(int comp, int idx, float, float, T& c0, T& c1, T& c2, T& u1, T& u2) const {
     c0 = c[comp][0][idx];
     c1 = c[comp][1][idx];
     c2 = c[comp][2][idx];
     u1 = c1;
     u2 = c2;
   }
-  // CPsi of Psi element pi of a face slot (the reference's per-element array)
-  __device__ __forceinline__ T cpsi(const Face<T>& F, int slot, long long pi, T, T) const {
-    return F.cpsi[slot][pi];
+  __device__ __forceinline__ T cpsi(const Face<T>& F, int slot, int pi, T, T) const { return F.cpsi[slot][pi]; }
+  __device__ __forceinline__ float invk(int, int) const { return 1.f; }
+  // interior (kappa = 1) form split into the load and its use, for prefetching
+  struct Raw {
+    T a, b, c;
+  };
+  __device__ __forceinline__ Raw fetch(int comp, int idx) const {
+    return Raw{c[comp][0][idx], c[comp][1][idx], c[comp][2][idx]};
+  }
+  __device__ __forceinline__ void decode(int, const Raw& r, T& c0, T& c1, T& c2) const {
+    c0 = r.a;
+    c1 = r.b;
+    c2 = r.c;
   }
 };
 
 constexpr int kTableRows = 256;
 
 struct TableCoef {
+  static constexpr bool kTable = true;
   const unsigned char* ids[6];  // per component, field order
-  const float* tab;             // [6][kTableRows][3] self, curl1, curl2 without kappa
-  const float* invk[6];         // 1/kappa along x y z for E (0..2) and H (3..5), length n+1
-  float d[3];                   // dx dy dz (CPsi = coefficient * cell size)
-  // positions along the curl axes: pos1 / pos2 are passed by the kernel
-  __device__ __forceinline__ void get(int comp, long long idx, int pos1, int pos2, float& c0, float& c1,
-                                      float& c2, float& u1, float& u2) const {
+  const float4* tab;            // [6][kTableRows] (self, curl1, curl2, 0) without kappa
+  const float* inv[6];          // 1/kappa along x y z for E (0..2) and H (3..5), length n+1
+  __device__ __forceinline__ void get(int comp, int idx, float k1, float k2, float& c0, float& c1, float& c2,
+                                      float& u1, float& u2) const {
     const int id = __ldg(ids[comp] + idx);
-    const float* r = tab + (comp * kTableRows + id) * 3;
-    c0 = __ldg(r);
-    u1 = __ldg(r + 1);
-    u2 = __ldg(r + 2);
-    // axis of curl1 / curl2 per component (see table above)
-    const int ax1 = comp == 0 ? 2 : comp == 1 ? 0 : comp == 2 ? 1 : comp == 3 ? 1 : comp == 4 ? 2 : 0;
-    const int ax2 = comp == 0 ? 1 : comp == 1 ? 2 : comp == 2 ? 0 : comp == 3 ? 2 : comp == 4 ? 0 : 1;
-    const int base = comp < 3 ? 3 : 0;
-    c1 = u1 * __ldg(invk[base + ax1] + pos1);
-    c2 = u2 * __ldg(invk[base + ax2] + pos2);
+    const float4 r = __ldg(tab + comp * kTableRows + id);
+    c0 = r.x;
+    u1 = r.y;
+    u2 = r.z;
+    c1 = u1 * k1;
+    c2 = u2 * k2;
   }
-  __device__ __forceinline__ float cpsi(const Face<float>& F, int, long long, float u, float dcell) const {
-    return u * dcell;
+  __device__ __forceinline__ float cpsi(const Face<float>&, int, int, float u, float dcell) const { return u * dcell; }
+  // 1/kappa of E (h=0) or H (h=1) at position pos along axis a
+  __device__ __forceinline__ float invk(int ha, int pos) const { return __ldg(inv[ha] + pos); }
+  // interior (kappa = 1) form split into the id load and the row lookup
+  using Raw = unsigned char;
+  __device__ __forceinline__ Raw fetch(int comp, int idx) const { return __ldg(ids[comp] + idx); }
+  __device__ __forceinline__ void decode(int comp, Raw id, float& c0, float& c1, float& c2) const {
+    const float4 r = __ldg(tab + comp * kTableRows + id);
+    c0 = r.x;
+    c1 = r.y;
+    c2 = r.z;
   }
 };
 
@@ -116,104 +136,249 @@ struct StepParams {
   int* ts;   // device step counter (index of the step being computed)
   Sources<T> src;
   T dcell[3];
+  int ichunk;  // x planes per thread
 };
 
-// CPML on one face for an H value: Psi update from `drive`, then H += CPsi*Psi.
-template <typename T, class C, bool EXACT>
-__device__ __forceinline__ void cpml_h(const C& coef, const Face<T>& F, int pos, long long pi_base,
-                                       long long pi_stride_ci, int slot, T drive, T u, T dcell, T& h) {
-  if (F.nc > 0 && pos >= F.m_start && pos < F.m_start + F.nc) {
-    const int ci = pos - F.m_start;
-    const long long pi = pi_base + (long long)ci * pi_stride_ci;
-    T* P = F.psi[slot];
-    const T ps = Ar<T, EXACT>::lin2(F.b_m[ci], P[pi], F.a_m[ci], drive);
-    P[pi] = ps;
-    h = Ar<T, EXACT>::axpy(h, coef.cpsi(F, slot, pi, u, dcell), ps);
-  }
+// Band of a face that contains `pos` (H: m band, E: e band): ci or -1.
+template <typename T>
+__device__ __forceinline__ int band_ci(const Face<T>& F, int pos, bool electric) {
+  const int st = electric ? F.e_start : F.m_start;
+  return (F.nc > 0 && pos >= st && pos < st + F.nc) ? pos - st : -1;
 }
 
-template <typename T, class C, bool EXACT>
-__device__ __forceinline__ void cpml_e(const C& coef, const Face<T>& F, int pos, long long pi_base,
-                                       long long pi_stride_ci, int slot, T drive, T u, T dcell, T& e) {
-  if (F.nc > 0 && pos >= F.e_start && pos < F.e_start + F.nc) {
-    const int ci = pos - F.e_start;
-    const long long pi = pi_base + (long long)ci * pi_stride_ci;
-    T* P = F.psi[slot];
-    const T ps = Ar<T, EXACT>::lin2(F.b_e[ci], P[pi], F.a_e[ci], drive);
-    P[pi] = ps;
-    e = Ar<T, EXACT>::axpy(e, coef.cpsi(F, slot, pi, u, dcell), ps);
+// One face's CPML on a value: Psi = b Psi + a drive, then v += CPsi Psi.
+template <typename T, class C, bool EXACT, bool ELECTRIC>
+__device__ __forceinline__ void cpml_apply(const C& coef, const Face<T>& F, int ci, int pi, int slot, T drive, T u,
+                                           T dcell, T& v) {
+  T* P = F.psi[slot];
+  const T b = ELECTRIC ? F.b_e[ci] : F.b_m[ci];
+  const T a = ELECTRIC ? F.a_e[ci] : F.a_m[ci];
+  const T ps = Ar<T, EXACT>::lin2(b, P[pi], a, drive);
+  P[pi] = ps;
+  v = Ar<T, EXACT>::axpy(v, coef.cpsi(F, slot, pi, u, dcell), ps);
+}
+
+// Source boxes that contain this thread's (j, k) for component `comp` (bit mask).
+template <typename T>
+__device__ __forceinline__ unsigned source_columns(const Sources<T>& s, int comp, int j, int k) {
+  unsigned m = 0;
+  for (int q = 0; q < s.n; q++) {
+    const SourceBox& b = s.box[q];
+    if (b.comp == comp && j >= b.j0 && j <= b.j1 && k >= b.k0 && k <= b.k1) m |= 1u << q;
   }
+  return m;
 }
 
 template <typename T>
-__device__ __forceinline__ bool in_e_band(const Face<T>& F, int pos) {
-  return F.nc > 0 && pos >= F.e_start && pos < F.e_start + F.nc;
+__device__ __forceinline__ void inject_masked(const Sources<T>& s, unsigned mask, int i, int j, int k, int ts, T& e) {
+  for (int q = 0; q < s.n; q++) {
+    if (!(mask >> q & 1u)) continue;
+    const SourceBox& b = s.box[q];
+    if (i < b.i0 || i > b.i1) continue;
+    const int ni = b.i1 - b.i0 + 1, nj = b.j1 - b.j0 + 1;
+    const int n = ((k - b.k0) * nj + (j - b.j0)) * ni + (i - b.i0);
+    e = add(e, mul(s.cs[q][n], s.wave[q][ts]));
+  }
 }
 
 // ---------------------------------------------------------------------------
 // H half-step
 // ---------------------------------------------------------------------------
-template <typename T, class C, bool EXACT>
-__global__ void __launch_bounds__(256) k_step_h(StepParams<T, C> p) {
-  using A = Ar<T, EXACT>;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z * blockDim.z + threadIdx.z;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0 &&
-      threadIdx.z == 0)
-    *p.ts += 1;  // first kernel of a step advances the device step counter
-  const GridDims& g = p.g;
-  if (i > g.nx || j > g.ny || k > g.nz) return;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
-  const Fields<T>& f = p.f;
-  T c0, c1, c2, u1, u2;
+// What a thread knows about its (j, k) column.
+template <typename T>
+struct HCol {
+  int j, k, oa, ob;                // column offsets: j*nz+k (Hx Hy Ez), j*(nz+1)+k (Hz Ey Ex)
+  bool hx_ok, hy_ok, hz_ok;        // which H components have this column
+  int yn, yp, zn, zp;              // H-band cell of the y/z faces, or -1
+  float kmy, kmz;                  // 1/kappa_m along y and z (table problems)
+};
 
+// H update of plane i of a column.  LEAN: no CPML band touches this plane of
+// the warp's columns, so the band tests and corrections are compiled out (and
+// every 1/kappa factor is exactly 1, so LEAN and full agree bit for bit).
+template <typename T, class C, bool EXACT, bool LEAN>
+__device__ __forceinline__ void h_plane(const StepParams<T, C>& p, const HCol<T>& c, int i, T& ez_c, T& ey_c) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  const bool inx = i < nx;
+  const T ez_n = (inx && c.hy_ok) ? f.Ez[(i + 1) * sHyEz + c.oa] : T(0);
+  const T ey_n = (inx && c.hz_ok) ? f.Ey[(i + 1) * sHzEy + c.ob] : T(0);
+  const int xn = LEAN ? -1 : band_ci(p.face[0], i, false), xp = LEAN ? -1 : band_ci(p.face[1], i, false);
+  const float kmx = LEAN ? 1.f : p.coef.invk(3, i);
+  const T dx = p.dcell[0], dy = p.dcell[1], dz = p.dcell[2];
+  T c0, c1, c2, u1, u2;
   // Hx (nx+1, ny, nz)
-  if (j < ny && k < nz) {
-    const long long idx = ((long long)i * ny + j) * nz + k;
-    const long long ey = ((long long)i * ny + j) * nzp1 + k;
-    const long long ez = ((long long)i * nyp1 + j) * nz + k;
-    const T dey = A::dif(f.Ey[ey + 1], f.Ey[ey]);
-    const T dez = A::dif(f.Ez[ez + nz], f.Ez[ez]);
-    p.coef.get(0, idx, k, j, c0, c1, c2, u1, u2);
+  if (c.hx_ok) {
+    const int idx = i * sHx + c.oa;
+    const T dey = A::dif(f.Ey[i * sHzEy + c.ob + 1], ey_c);
+    const T dez = A::dif(f.Ez[i * sHyEz + c.oa + nz], ez_c);
+    p.coef.get(0, idx, c.kmz, c.kmy, c0, c1, c2, u1, u2);
     T h = A::lin3(c0, f.Hx[idx], c1, dey, c2, dez);
-    // y faces: Psi_hxy (nx+1, nc, nz) by dEz/dy; z faces: Psi_hxz (nx+1, ny, nc) by dEy/dz
-    cpml_h<T, C, EXACT>(p.coef, p.face[2], j, (long long)i * p.face[2].nc * nz + k, nz, 0, dez, u2, p.dcell[1], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[3], j, (long long)i * p.face[3].nc * nz + k, nz, 0, dez, u2, p.dcell[1], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[4], k, ((long long)i * ny + j) * p.face[4].nc, 1, 0, dey, u1, p.dcell[2], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[5], k, ((long long)i * ny + j) * p.face[5].nc, 1, 0, dey, u1, p.dcell[2], h);
+    if (!LEAN) {
+      // y faces: Psi_hxy (nx+1, nc, nz) by dEz/dy; z faces: Psi_hxz (nx+1, ny, nc) by dEy/dz
+      if (c.yn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[2], c.yn, (i * p.face[2].nc + c.yn) * nz + c.k, 0, dez, u2, dy, h);
+      if (c.yp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[3], c.yp, (i * p.face[3].nc + c.yp) * nz + c.k, 0, dez, u2, dy, h);
+      if (c.zn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[4], c.zn, (i * ny + c.j) * p.face[4].nc + c.zn, 0, dey, u1, dz, h);
+      if (c.zp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[5], c.zp, (i * ny + c.j) * p.face[5].nc + c.zp, 0, dey, u1, dz, h);
+    }
     f.Hx[idx] = h;
   }
-  // Hy (nx, ny+1, nz)
-  if (i < nx && k < nz) {
-    const long long idx = ((long long)i * nyp1 + j) * nz + k;
-    const long long ex = ((long long)i * nyp1 + j) * nzp1 + k;
-    const T dez = A::dif(f.Ez[idx + (long long)nyp1 * nz], f.Ez[idx]);  // Ez shares Hy's (j,k) layout
-    const T dex = A::dif(f.Ex[ex + 1], f.Ex[ex]);
-    p.coef.get(1, idx, i, k, c0, c1, c2, u1, u2);
-    T h = A::lin3(c0, f.Hy[idx], c1, dez, c2, dex);
-    // x faces: Psi_hyx (nc, ny+1, nz) by dEz/dx; z faces: Psi_hyz (nx, ny+1, nc) by dEx/dz
-    cpml_h<T, C, EXACT>(p.coef, p.face[0], i, (long long)j * nz + k, (long long)nyp1 * nz, 0, dez, u1, p.dcell[0], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[1], i, (long long)j * nz + k, (long long)nyp1 * nz, 0, dez, u1, p.dcell[0], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[4], k, ((long long)i * nyp1 + j) * p.face[4].nc, 1, 1, dex, u2, p.dcell[2], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[5], k, ((long long)i * nyp1 + j) * p.face[5].nc, 1, 1, dex, u2, p.dcell[2], h);
-    f.Hy[idx] = h;
+  if (inx) {
+    const int ex = i * sEx + c.ob;
+    const T ex_c = f.Ex[ex];
+    // Hy (nx, ny+1, nz)
+    if (c.hy_ok) {
+      const int idx = i * sHyEz + c.oa;
+      const T dez = A::dif(ez_n, ez_c);
+      const T dex = A::dif(f.Ex[ex + 1], ex_c);
+      p.coef.get(1, idx, kmx, c.kmz, c0, c1, c2, u1, u2);
+      T h = A::lin3(c0, f.Hy[idx], c1, dez, c2, dex);
+      if (!LEAN) {
+        // x faces: Psi_hyx (nc, ny+1, nz) by dEz/dx; z faces: Psi_hyz (nx, ny+1, nc) by dEx/dz
+        if (xn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[0], xn, xn * sHyEz + c.oa, 0, dez, u1, dx, h);
+        if (xp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[1], xp, xp * sHyEz + c.oa, 0, dez, u1, dx, h);
+        if (c.zn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[4], c.zn, (i * nyp1 + c.j) * p.face[4].nc + c.zn, 1, dex, u2, dz, h);
+        if (c.zp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[5], c.zp, (i * nyp1 + c.j) * p.face[5].nc + c.zp, 1, dex, u2, dz, h);
+      }
+      f.Hy[idx] = h;
+    }
+    // Hz (nx, ny, nz+1)
+    if (c.hz_ok) {
+      const int idx = i * sHzEy + c.ob;
+      const T dex = A::dif(f.Ex[ex + nzp1], ex_c);
+      const T dey = A::dif(ey_n, ey_c);
+      p.coef.get(2, idx, c.kmy, kmx, c0, c1, c2, u1, u2);
+      T h = A::lin3(c0, f.Hz[idx], c1, dex, c2, dey);
+      if (!LEAN) {
+        // x faces: Psi_hzx (nc, ny, nz+1) by dEy/dx; y faces: Psi_hzy (nx, nc, nz+1) by dEx/dy
+        if (xn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[0], xn, xn * sHzEy + c.ob, 1, dey, u2, dx, h);
+        if (xp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[1], xp, xp * sHzEy + c.ob, 1, dey, u2, dx, h);
+        if (c.yn >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[2], c.yn, (i * p.face[2].nc + c.yn) * nzp1 + c.k, 1, dex, u1, dy, h);
+        if (c.yp >= 0) cpml_apply<T, C, EXACT, false>(p.coef, p.face[3], c.yp, (i * p.face[3].nc + c.yp) * nzp1 + c.k, 1, dex, u1, dy, h);
+      }
+      f.Hz[idx] = h;
+    }
   }
-  // Hz (nx, ny, nz+1)
-  if (i < nx && j < ny) {
-    const long long idx = ((long long)i * ny + j) * nzp1 + k;
-    const long long ex = ((long long)i * nyp1 + j) * nzp1 + k;
-    const T dex = A::dif(f.Ex[ex + nzp1], f.Ex[ex]);
-    const T dey = A::dif(f.Ey[idx + (long long)ny * nzp1], f.Ey[idx]);  // Ey shares Hz's (j,k) layout
-    p.coef.get(2, idx, j, i, c0, c1, c2, u1, u2);
-    T h = A::lin3(c0, f.Hz[idx], c1, dex, c2, dey);
-    // x faces: Psi_hzx (nc, ny, nz+1) by dEy/dx; y faces: Psi_hzy (nx, nc, nz+1) by dEx/dy
-    cpml_h<T, C, EXACT>(p.coef, p.face[0], i, (long long)j * nzp1 + k, (long long)ny * nzp1, 1, dey, u2, p.dcell[0], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[1], i, (long long)j * nzp1 + k, (long long)ny * nzp1, 1, dey, u2, p.dcell[0], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[2], j, (long long)i * p.face[2].nc * nzp1 + k, nzp1, 1, dex, u1, p.dcell[1], h);
-    cpml_h<T, C, EXACT>(p.coef, p.face[3], j, (long long)i * p.face[3].nc * nzp1 + k, nzp1, 1, dex, u1, p.dcell[1], h);
-    f.Hz[idx] = h;
+  ez_c = ez_n;
+  ey_c = ey_n;
+}
+
+// Inputs of one interior plane of an H column, loaded one plane ahead.
+template <typename T, class C>
+struct HIn {
+  T hx, hy, hz, ey_kp, ez_jp, ex, ex_kp, ex_jp, ez_n, ey_n;
+  typename C::Raw r0, r1, r2;
+};
+
+template <typename T, class C>
+__device__ __forceinline__ void h_load(const StepParams<T, C>& p, const HCol<T>& c, int i, HIn<T, C>& in) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  const int ex = i * sEx + c.ob;
+  in.ex = f.Ex[ex];
+  if (c.hx_ok) {
+    const int idx = i * sHx + c.oa;
+    in.hx = f.Hx[idx];
+    in.ey_kp = f.Ey[i * sHzEy + c.ob + 1];
+    in.ez_jp = f.Ez[i * sHyEz + c.oa + nz];
+    in.r0 = p.coef.fetch(0, idx);
   }
+  if (c.hy_ok) {
+    const int idx = i * sHyEz + c.oa;
+    in.hy = f.Hy[idx];
+    in.ex_kp = f.Ex[ex + 1];
+    in.ez_n = f.Ez[idx + sHyEz];
+    in.r1 = p.coef.fetch(1, idx);
+  }
+  if (c.hz_ok) {
+    const int idx = i * sHzEy + c.ob;
+    in.hz = f.Hz[idx];
+    in.ex_jp = f.Ex[ex + nzp1];
+    in.ey_n = f.Ey[idx + sHzEy];
+    in.r2 = p.coef.fetch(2, idx);
+  }
+}
+
+// Interior H plane (no CPML, kappa = 1): the same operations as h_plane<LEAN>.
+template <typename T, class C, bool EXACT>
+__device__ __forceinline__ void h_store(const StepParams<T, C>& p, const HCol<T>& c, int i, const HIn<T, C>& in,
+                                        T& ez_c, T& ey_c) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1;
+  const Fields<T>& f = p.f;
+  T c0, c1, c2;
+  if (c.hx_ok) {
+    p.coef.decode(0, in.r0, c0, c1, c2);
+    f.Hx[i * sHx + c.oa] = A::lin3(c0, in.hx, c1, A::dif(in.ey_kp, ey_c), c2, A::dif(in.ez_jp, ez_c));
+  }
+  if (c.hy_ok) {
+    p.coef.decode(1, in.r1, c0, c1, c2);
+    f.Hy[i * sHyEz + c.oa] = A::lin3(c0, in.hy, c1, A::dif(in.ez_n, ez_c), c2, A::dif(in.ex_kp, in.ex));
+  }
+  if (c.hz_ok) {
+    p.coef.decode(2, in.r2, c0, c1, c2);
+    f.Hz[i * sHzEy + c.ob] = A::lin3(c0, in.hz, c1, A::dif(in.ex_jp, in.ex), c2, A::dif(in.ey_n, ey_c));
+  }
+  ez_c = in.ez_n;
+  ey_c = in.ey_n;
+}
+
+template <typename T, class C, bool EXACT>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_h(StepParams<T, C> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i0 = blockIdx.z * p.ichunk;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+    *p.ts += 1;  // first kernel of a step advances the device step counter
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
+  const bool valid = j <= ny && k <= nz;
+  HCol<T> c;
+  c.j = j;
+  c.k = k;
+  c.oa = j * nz + k;
+  c.ob = j * (nz + 1) + k;
+  c.hx_ok = j < ny && k < nz;
+  c.hy_ok = k < nz;
+  c.hz_ok = j < ny;
+  c.yn = band_ci(p.face[2], j, false);
+  c.yp = band_ci(p.face[3], j, false);
+  c.zn = band_ci(p.face[4], k, false);
+  c.zp = band_ci(p.face[5], k, false);
+  // a warp is 32 consecutive k of one j: it takes the lean path when none of
+  // its columns lies in a y or z band
+  const bool lean_col = !valid || (c.yn < 0 && c.yp < 0 && c.zn < 0 && c.zp < 0);
+  const bool warp_lean = __all_sync(0xffffffffu, lean_col);
+  if (!valid) return;
+  c.kmy = p.coef.invk(4, j);
+  c.kmz = p.coef.invk(5, k);
+  const int i1 = min(i0 + p.ichunk, nx + 1);
+  // carried x-neighbours: Ez(i,j,k), Ey(i,j,k)
+  T ez_c = c.hy_ok ? p.f.Ez[i0 * (ny + 1) * nz + c.oa] : T(0);
+  T ey_c = c.hz_ok ? p.f.Ey[i0 * ny * (nz + 1) + c.ob] : T(0);
+  // interior planes [xa, xb): outside both x bands and below nx
+  int xa = i1, xb = i1;
+  if (warp_lean) {
+    const int lo = p.face[0].nc > 0 ? p.face[0].m_start + p.face[0].nc : 0;
+    const int hi = p.face[1].nc > 0 ? p.face[1].m_start : nx;
+    xa = min(max(i0, lo), i1);
+    xb = max(xa, min(i1, hi));
+  }
+  for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+  if (xa < xb) {
+    // software pipeline: plane i+1's loads are in flight while plane i is computed and stored
+    HIn<T, C> cur, nxt;
+    h_load(p, c, xa, cur);
+    for (int i = xa; i < xb; i++) {
+      if (i + 1 < xb) h_load(p, c, i + 1, nxt);
+      h_store<T, C, EXACT>(p, c, i, cur, ez_c, ey_c);
+      cur = nxt;
+    }
+  }
+  for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
 }
 
 // ---------------------------------------------------------------------------
@@ -223,19 +388,18 @@ template <typename T, class C, bool EXACT>
 __global__ void __launch_bounds__(256) k_step_mid(StepParams<T, C> p, Probes probes) {
   using A = Ar<T, EXACT>;
   const int ts = *p.ts;
-  const GridDims& g = p.g;
-  const int ny = g.ny, nz = g.nz, nzp1 = nz + 1;
+  const int ny = p.g.ny, nz = p.g.nz, nzp1 = nz + 1;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long plane = (long long)ny * nzp1;
   if (t < plane) {
     const int j = (int)(t / nzp1), k = (int)(t % nzp1);
-    const long long idx = (long long)j * nzp1 + k;  // Ex(0, j, k)
+    const int idx = j * nzp1 + k;  // Ex(0, j, k)
     T e = p.f.Ex[idx];
     if (j >= 1 && k >= 1 && k < nz) {
-      const T dhz = A::dif(p.f.Hz[(long long)j * nzp1 + k], p.f.Hz[(long long)(j - 1) * nzp1 + k]);
-      const T dhy = A::dif(p.f.Hy[(long long)j * nz + k], p.f.Hy[(long long)j * nz + k - 1]);
+      const T dhz = A::dif(p.f.Hz[j * nzp1 + k], p.f.Hz[(j - 1) * nzp1 + k]);
+      const T dhy = A::dif(p.f.Hy[j * nz + k], p.f.Hy[j * nz + k - 1]);
       T c0, c1, c2, u1, u2;
-      p.coef.get(3, idx, j, k, c0, c1, c2, u1, u2);
+      p.coef.get(3, idx, p.coef.invk(1, j), p.coef.invk(2, k), c0, c1, c2, u1, u2);
       e = A::lin3(c0, e, c1, dhz, c2, dhy);
     }
     p.ex0b[idx] = e;
@@ -247,85 +411,207 @@ __global__ void __launch_bounds__(256) k_step_mid(StepParams<T, C> p, Probes pro
 // ---------------------------------------------------------------------------
 // E half-step
 // ---------------------------------------------------------------------------
-template <typename T, class C, bool EXACT>
-__global__ void __launch_bounds__(256) k_step_e(StepParams<T, C> p) {
-  using A = Ar<T, EXACT>;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z * blockDim.z + threadIdx.z;
-  const GridDims& g = p.g;
-  if (i > g.nx || j > g.ny || k > g.nz) return;
-  const int ts = *p.ts;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
-  const Fields<T>& f = p.f;
-  T c0, c1, c2, u1, u2;
+template <typename T>
+struct ECol {
+  int j, k, oa, ob;
+  bool jy, kz, ey_ok, ez_ok;       // interior in y / z, Ey / Ez exist in this column
+  int yn, yp, zn, zp;              // E-band cell of the y/z faces, or -1
+  float key, kez;                  // 1/kappa_e along y and z (table problems)
+  unsigned sx, sy, sz;             // sources covering this column (Ex, Ey, Ez)
+};
 
-  // Ex (nx, ny+1, nz+1): bulk on j in [1,ny), k in [1,nz); y-face and z-face CPML
-  if (i < nx) {
-    const long long idx = ((long long)i * nyp1 + j) * nzp1 + k;
+template <typename T, class C, bool EXACT, bool LEAN>
+__device__ __forceinline__ void e_plane(const StepParams<T, C>& p, const ECol<T>& c, int i, int ts, T& hz_p, T& hy_p) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  const bool inx = i < nx;
+  // Hz(i,j,k) and Hy(i,j,k); at i = nx the reference reads Ex(0,j,k) after its
+  // bulk update and the start of the Hz array instead (one plane past Hz / Hy)
+  T hz_i = T(0), hy_i = T(0);
+  if (c.ey_ok) hz_i = inx ? f.Hz[i * sHzEy + c.ob] : p.ex0b[c.ob];
+  if (c.ez_ok) hy_i = inx ? f.Hy[i * sHyEz + c.oa] : f.Hz[c.oa];
+  const int xn = LEAN ? -1 : band_ci(p.face[0], i, true), xp = LEAN ? -1 : band_ci(p.face[1], i, true);
+  const float kex = LEAN ? 1.f : p.coef.invk(0, i);
+  const T hx_c = (c.ey_ok && c.ez_ok) ? f.Hx[i * sHx + c.oa] : T(0);
+  const T dx = p.dcell[0], dy = p.dcell[1], dz = p.dcell[2];
+  T c0, c1, c2, u1, u2;
+  // Ex (nx, ny+1, nz+1): bulk on j in [1,ny), k in [1,nz)
+  if (inx) {
+    const int idx = i * sEx + c.ob;
     T e = f.Ex[idx];
-    const bool jy = (j >= 1 && j < ny), kz = (k >= 1 && k < nz);
     T dhz = T(0), dhy = T(0);
-    if (jy) dhz = A::dif(f.Hz[((long long)i * ny + j) * nzp1 + k], f.Hz[((long long)i * ny + j - 1) * nzp1 + k]);
-    if (kz) dhy = A::dif(f.Hy[((long long)i * nyp1 + j) * nz + k], f.Hy[((long long)i * nyp1 + j) * nz + k - 1]);
-    p.coef.get(3, idx, j, k, c0, c1, c2, u1, u2);
-    if (jy && kz) e = A::lin3(c0, e, c1, dhz, c2, dhy);
-    // y faces: Psi_exy (nx, nc, nz+1) by dHz/dy; z faces: Psi_exz (nx, ny+1, nc) by dHy/dz
-    cpml_e<T, C, EXACT>(p.coef, p.face[2], j, (long long)i * p.face[2].nc * nzp1 + k, nzp1, 3, dhz, u1, p.dcell[1], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[3], j, (long long)i * p.face[3].nc * nzp1 + k, nzp1, 3, dhz, u1, p.dcell[1], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[4], k, ((long long)i * nyp1 + j) * p.face[4].nc, 1, 2, dhy, u2, p.dcell[2], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[5], k, ((long long)i * nyp1 + j) * p.face[5].nc, 1, 2, dhy, u2, p.dcell[2], e);
-    inject_sources(p.src, 0, i, j, k, ts, e);
+    if (c.jy) dhz = A::dif(hz_i, f.Hz[i * sHzEy + c.ob - nzp1]);
+    if (c.kz) dhy = A::dif(hy_i, f.Hy[i * sHyEz + c.oa - 1]);
+    p.coef.get(3, idx, c.key, c.kez, c0, c1, c2, u1, u2);
+    if (c.jy && c.kz) e = A::lin3(c0, e, c1, dhz, c2, dhy);
+    if (!LEAN) {
+      // y faces: Psi_exy (nx, nc, nz+1) by dHz/dy; z faces: Psi_exz (nx, ny+1, nc) by dHy/dz
+      if (c.yn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[2], c.yn, (i * p.face[2].nc + c.yn) * nzp1 + c.k, 3, dhz, u1, dy, e);
+      if (c.yp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[3], c.yp, (i * p.face[3].nc + c.yp) * nzp1 + c.k, 3, dhz, u1, dy, e);
+      if (c.zn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[4], c.zn, (i * nyp1 + c.j) * p.face[4].nc + c.zn, 2, dhy, u2, dz, e);
+      if (c.zp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[5], c.zp, (i * nyp1 + c.j) * p.face[5].nc + c.zp, 2, dhy, u2, dz, e);
+      if (c.sx) inject_masked(p.src, c.sx, i, c.j, c.k, ts, e);
+    }
     f.Ex[idx] = e;
   }
-  // Ey (nx+1, ny, nz+1): bulk on i in [1,nx], k in [1,nz); x-face and z-face CPML
-  if (j < ny) {
-    const long long idx = ((long long)i * ny + j) * nzp1 + k;
+  // Ey (nx+1, ny, nz+1): bulk on i in [1,nx], k in [1,nz)
+  if (c.ey_ok) {
+    const int idx = i * sHzEy + c.ob;
     T e = f.Ey[idx];
-    const bool kz = (k >= 1 && k < nz);
-    const bool bulk = (i >= 1) && kz;
-    const bool xb = in_e_band(p.face[0], i) || in_e_band(p.face[1], i);
     T dhx = T(0), dhz = T(0);
-    if (kz) dhx = A::dif(f.Hx[((long long)i * ny + j) * nz + k], f.Hx[((long long)i * ny + j) * nz + k - 1]);
-    if (bulk || xb) {
-      // Hz(i=nx) does not exist; the reference reads Ex(0,j,k) there, after its bulk update
-      const T hz1 = (i < nx) ? f.Hz[idx] : p.ex0b[(long long)j * nzp1 + k];  // Hz shares Ey's (j,k) layout
-      dhz = A::dif(hz1, f.Hz[idx - (long long)ny * nzp1]);
+    if (c.kz) dhx = A::dif(hx_c, f.Hx[i * sHx + c.oa - 1]);
+    if (i >= 1) dhz = A::dif(hz_i, hz_p);
+    p.coef.get(4, idx, c.kez, kex, c0, c1, c2, u1, u2);
+    if (i >= 1 && c.kz) e = A::lin3(c0, e, c1, dhx, c2, dhz);
+    if (!LEAN) {
+      // x faces: Psi_eyx (nc, ny, nz+1) by dHz/dx; z faces: Psi_eyz (nx+1, ny, nc) by dHx/dz
+      if (xn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[0], xn, xn * sHzEy + c.ob, 2, dhz, u2, dx, e);
+      if (xp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[1], xp, xp * sHzEy + c.ob, 2, dhz, u2, dx, e);
+      if (c.zn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[4], c.zn, (i * ny + c.j) * p.face[4].nc + c.zn, 3, dhx, u1, dz, e);
+      if (c.zp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[5], c.zp, (i * ny + c.j) * p.face[5].nc + c.zp, 3, dhx, u1, dz, e);
+      if (c.sy) inject_masked(p.src, c.sy, i, c.j, c.k, ts, e);
     }
-    p.coef.get(4, idx, k, i, c0, c1, c2, u1, u2);
-    if (bulk) e = A::lin3(c0, e, c1, dhx, c2, dhz);
-    // x faces: Psi_eyx (nc, ny, nz+1) by dHz/dx; z faces: Psi_eyz (nx+1, ny, nc) by dHx/dz
-    cpml_e<T, C, EXACT>(p.coef, p.face[0], i, (long long)j * nzp1 + k, (long long)ny * nzp1, 2, dhz, u2, p.dcell[0], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[1], i, (long long)j * nzp1 + k, (long long)ny * nzp1, 2, dhz, u2, p.dcell[0], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[4], k, ((long long)i * ny + j) * p.face[4].nc, 1, 3, dhx, u1, p.dcell[2], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[5], k, ((long long)i * ny + j) * p.face[5].nc, 1, 3, dhx, u1, p.dcell[2], e);
-    inject_sources(p.src, 1, i, j, k, ts, e);
     f.Ey[idx] = e;
   }
-  // Ez (nx+1, ny+1, nz): bulk on i in [1,nx], j in [1,ny); x-face and y-face CPML
-  if (k < nz) {
-    const long long idx = ((long long)i * nyp1 + j) * nz + k;
+  // Ez (nx+1, ny+1, nz): bulk on i in [1,nx], j in [1,ny)
+  if (c.ez_ok) {
+    const int idx = i * sHyEz + c.oa;
     T e = f.Ez[idx];
-    const bool jy = (j >= 1 && j < ny);
-    const bool bulk = (i >= 1) && jy;
-    const bool xb = in_e_band(p.face[0], i) || in_e_band(p.face[1], i);
     T dhy = T(0), dhx = T(0);
-    if (bulk || xb) {
-      // Hy(i=nx) does not exist; the reference reads the Hz array from its start there
-      const T hy1 = (i < nx) ? f.Hy[idx] : f.Hz[(long long)j * nz + k];  // Hy shares Ez's (j,k) layout
-      dhy = A::dif(hy1, f.Hy[idx - (long long)nyp1 * nz]);
+    if (i >= 1) dhy = A::dif(hy_i, hy_p);
+    if (c.jy) dhx = A::dif(hx_c, f.Hx[i * sHx + c.oa - nz]);
+    p.coef.get(5, idx, kex, c.key, c0, c1, c2, u1, u2);
+    if (i >= 1 && c.jy) e = A::lin3(c0, e, c1, dhy, c2, dhx);
+    if (!LEAN) {
+      // x faces: Psi_ezx (nc, ny+1, nz) by dHy/dx; y faces: Psi_ezy (nx+1, nc, nz) by dHx/dy
+      if (xn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[0], xn, xn * sHyEz + c.oa, 3, dhy, u1, dx, e);
+      if (xp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[1], xp, xp * sHyEz + c.oa, 3, dhy, u1, dx, e);
+      if (c.yn >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[2], c.yn, (i * p.face[2].nc + c.yn) * nz + c.k, 2, dhx, u2, dy, e);
+      if (c.yp >= 0) cpml_apply<T, C, EXACT, true>(p.coef, p.face[3], c.yp, (i * p.face[3].nc + c.yp) * nz + c.k, 2, dhx, u2, dy, e);
+      if (c.sz) inject_masked(p.src, c.sz, i, c.j, c.k, ts, e);
     }
-    if (jy) dhx = A::dif(f.Hx[((long long)i * ny + j) * nz + k], f.Hx[((long long)i * ny + j - 1) * nz + k]);
-    p.coef.get(5, idx, i, j, c0, c1, c2, u1, u2);
-    if (bulk) e = A::lin3(c0, e, c1, dhy, c2, dhx);
-    // x faces: Psi_ezx (nc, ny+1, nz) by dHy/dx; y faces: Psi_ezy (nx+1, nc, nz) by dHx/dy
-    cpml_e<T, C, EXACT>(p.coef, p.face[0], i, (long long)j * nz + k, (long long)nyp1 * nz, 3, dhy, u1, p.dcell[0], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[1], i, (long long)j * nz + k, (long long)nyp1 * nz, 3, dhy, u1, p.dcell[0], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[2], j, (long long)i * p.face[2].nc * nz + k, nz, 2, dhx, u2, p.dcell[1], e);
-    cpml_e<T, C, EXACT>(p.coef, p.face[3], j, (long long)i * p.face[3].nc * nz + k, nz, 2, dhx, u2, p.dcell[1], e);
-    inject_sources(p.src, 2, i, j, k, ts, e);
     f.Ez[idx] = e;
   }
+  hz_p = hz_i;
+  hy_p = hy_i;
+}
+
+// Inputs of one interior plane (1 <= i < nx) of an E column, loaded one plane ahead.
+template <typename T, class C>
+struct EIn {
+  T ex, ey, ez, hz, hy, hz_jm, hy_km, hx, hx_km, hx_jm;
+  typename C::Raw r0, r1, r2;
+};
+
+template <typename T, class C>
+__device__ __forceinline__ void e_load(const StepParams<T, C>& p, const ECol<T>& c, int i, EIn<T, C>& in) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  if (c.jy && c.kz) {
+    const int idx = i * sEx + c.ob;
+    in.ex = f.Ex[idx];
+    in.r0 = p.coef.fetch(3, idx);
+  }
+  if (c.ey_ok) in.hz = f.Hz[i * sHzEy + c.ob];
+  if (c.ez_ok) in.hy = f.Hy[i * sHyEz + c.oa];
+  if (c.jy) in.hz_jm = f.Hz[i * sHzEy + c.ob - nzp1];
+  if (c.kz) in.hy_km = f.Hy[i * sHyEz + c.oa - 1];
+  if (c.ey_ok && c.ez_ok) in.hx = f.Hx[i * sHx + c.oa];
+  if (c.kz && c.ey_ok) {
+    const int idx = i * sHzEy + c.ob;
+    in.ey = f.Ey[idx];
+    in.hx_km = f.Hx[i * sHx + c.oa - 1];
+    in.r1 = p.coef.fetch(4, idx);
+  }
+  if (c.jy && c.ez_ok) {
+    const int idx = i * sHyEz + c.oa;
+    in.ez = f.Ez[idx];
+    in.hx_jm = f.Hx[i * sHx + c.oa - nz];
+    in.r2 = p.coef.fetch(5, idx);
+  }
+}
+
+// Interior E plane (no CPML, no source, 1 <= i < nx): the same operations as
+// e_plane<LEAN>; values that the bulk update leaves alone are not rewritten.
+template <typename T, class C, bool EXACT>
+__device__ __forceinline__ void e_store(const StepParams<T, C>& p, const ECol<T>& c, int i, const EIn<T, C>& in,
+                                        T& hz_p, T& hy_p) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  T c0, c1, c2;
+  if (c.jy && c.kz) {
+    p.coef.decode(3, in.r0, c0, c1, c2);
+    f.Ex[i * sEx + c.ob] = A::lin3(c0, in.ex, c1, A::dif(in.hz, in.hz_jm), c2, A::dif(in.hy, in.hy_km));
+  }
+  if (c.kz && c.ey_ok) {
+    p.coef.decode(4, in.r1, c0, c1, c2);
+    f.Ey[i * sHzEy + c.ob] = A::lin3(c0, in.ey, c1, A::dif(in.hx, in.hx_km), c2, A::dif(in.hz, hz_p));
+  }
+  if (c.jy && c.ez_ok) {
+    p.coef.decode(5, in.r2, c0, c1, c2);
+    f.Ez[i * sHyEz + c.oa] = A::lin3(c0, in.ez, c1, A::dif(in.hy, hy_p), c2, A::dif(in.hx, in.hx_jm));
+  }
+  hz_p = in.hz;
+  hy_p = in.hy;
+}
+
+template <typename T, class C, bool EXACT>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_e(StepParams<T, C> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i0 = blockIdx.z * p.ichunk;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
+  const bool valid = j <= ny && k <= nz;
+  ECol<T> c;
+  c.j = j;
+  c.k = k;
+  c.oa = j * nz + k;
+  c.ob = j * (nz + 1) + k;
+  c.jy = j >= 1 && j < ny;
+  c.kz = k >= 1 && k < nz;
+  c.ey_ok = j < ny;
+  c.ez_ok = k < nz;
+  c.yn = band_ci(p.face[2], j, true);
+  c.yp = band_ci(p.face[3], j, true);
+  c.zn = band_ci(p.face[4], k, true);
+  c.zp = band_ci(p.face[5], k, true);
+  c.sx = source_columns(p.src, 0, j, k);
+  c.sy = source_columns(p.src, 1, j, k);
+  c.sz = source_columns(p.src, 2, j, k);
+  const bool lean_col = !valid || (c.yn < 0 && c.yp < 0 && c.zn < 0 && c.zp < 0 && !(c.sx | c.sy | c.sz));
+  const bool warp_lean = __all_sync(0xffffffffu, lean_col);
+  if (!valid) return;
+  c.key = p.coef.invk(1, j);
+  c.kez = p.coef.invk(2, k);
+  const int ts = *p.ts;
+  const int i1 = min(i0 + p.ichunk, nx + 1);
+  // carried x-neighbours: Hz(i-1,j,k), Hy(i-1,j,k)
+  T hz_p = (i0 >= 1 && c.ey_ok) ? p.f.Hz[(i0 - 1) * ny * (nz + 1) + c.ob] : T(0);
+  T hy_p = (i0 >= 1 && c.ez_ok) ? p.f.Hy[(i0 - 1) * (ny + 1) * nz + c.oa] : T(0);
+  // interior planes [xa, xb): 1 <= i < nx and outside both x bands
+  int xa = i1, xb = i1;
+  if (warp_lean) {
+    const int lo = p.face[0].nc > 0 ? p.face[0].e_start + p.face[0].nc : 1;
+    const int hi = p.face[1].nc > 0 ? p.face[1].e_start : nx;
+    xa = min(max(i0, max(lo, 1)), i1);
+    xb = max(xa, min(i1, min(hi, nx)));
+  }
+  for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  if (xa < xb) {
+    EIn<T, C> cur, nxt;
+    e_load(p, c, xa, cur);
+    for (int i = xa; i < xb; i++) {
+      if (i + 1 < xb) e_load(p, c, i + 1, nxt);
+      e_store<T, C, EXACT>(p, c, i, cur, hz_p, hy_p);
+      cur = nxt;
+    }
+  }
+  for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
 }
 
 }  // namespace fdtd
