@@ -178,7 +178,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
-    ap.add_argument("--tune-steps", type=int, default=32, help="steps timed per autotuner candidate")
+    ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
@@ -264,7 +264,7 @@ def main():
     # --- device-timed run
     eng = Engine(prob, args.precision, device=local)
     if tuning:
-        autotune.set_tiling(eng, tuning["chunk"], tuning["rows"])
+        autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
     eng.run(W)
     barrier()
     with ClockSampler(local) as clk:
@@ -293,7 +293,7 @@ def main():
                      "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom],
                      "traffic": traffic},
         "kernel_ms": kern,
-        "tiling": {k: tuning[k] for k in ("chunk", "rows", "ms_per_step")} if tuning else "default",
+        "tiling": {k: tuning[k] for k in ("chunk", "rows", "prefetch", "ms_per_step")} if tuning else "default",
         "clocks": clk.summary(),
         "gpu_launches": 4 * K,
         "e2e": e2e,
@@ -333,9 +333,9 @@ def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
     from special_topics_b200.scenario import build_problem_from_scenario
     from special_topics_b200 import autotune
     p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=1000), 1000)
-    tuning = autotune.tune(p, "f64", steps_per_candidate=16)
+    tuning = autotune.tune(p, "f64", steps_per_candidate=8)
     eng = Engine(p, "f64")
-    autotune.set_tiling(eng, tuning["chunk"], tuning["rows"])
+    autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
     eng.run(W)
     ms = eng.run_timed(K)
     kern = eng.profile_kernels(8)
@@ -345,7 +345,7 @@ def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
     dom = "e" if kern["e"] >= kern["h"] else "h"
     ach = byts[dom] / (kern[dom] / 1e3) / 1e9
     return {"workload": f"scaling-box-{n[0]}x{n[1]}x{n[2]}", "value": p.grid.cells * K / (ms / 1e3) / 1e9,
-            "unit": "Gcell-updates/s", "ms_per_step": ms / K, "tiling": {"chunk": tuning["chunk"], "rows": tuning["rows"]},
+            "unit": "Gcell-updates/s", "ms_per_step": ms / K, "tiling": {k: tuning[k] for k in ("chunk", "rows", "prefetch")},
             "roofline": {"kernel": f"k_step_{dom}", "achieved": ach, "peak": peak, "frac": ach / peak}}
 
 

@@ -179,6 +179,9 @@ int fdtd_ctx_run(fdtd_ctx* ctx, int count);
  * autotuner (special-topics_b200/autotune.py) picks the fastest per grid. */
 int fdtd_ctx_set_tiling(fdtd_ctx* ctx, int x_planes_per_thread, int block_rows);
 int fdtd_ctx_get_tiling(const fdtd_ctx* ctx, int* x_planes_per_thread, int* block_rows);
+/* How many x planes ahead the interior loop of the step kernels loads (1 or 2);
+ * same results either way, chosen by the autotuner. */
+int fdtd_ctx_set_prefetch(fdtd_ctx* ctx, int planes);
 /* fdtd_ctx_run that also reports the device time (ms) between CUDA events
  * recorded on the handle's stream before the first and after the last launch. */
 int fdtd_ctx_run_timed(fdtd_ctx* ctx, int count, float* ms);

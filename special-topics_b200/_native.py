@@ -30,7 +30,7 @@ EXPORTS = (
     "fdtd_ctx_upload_cpml", "fdtd_ctx_add_vsource", "fdtd_ctx_add_svoltage", "fdtd_ctx_add_scurrent",
     "fdtd_ctx_setup_farfield", "fdtd_ctx_upload_material", "fdtd_ctx_build_material",
     "fdtd_ctx_override_material", "fdtd_ctx_read_material", "fdtd_ctx_run", "fdtd_ctx_run_timed",
-    "fdtd_ctx_profile_kernels", "fdtd_ctx_set_tiling", "fdtd_ctx_get_tiling", "fdtd_ctx_step", "fdtd_status",
+    "fdtd_ctx_profile_kernels", "fdtd_ctx_set_tiling", "fdtd_ctx_get_tiling", "fdtd_ctx_set_prefetch", "fdtd_ctx_step", "fdtd_status",
     "fdtd_ctx_read_trace", "fdtd_ctx_read_field", "fdtd_ctx_read_psi", "fdtd_ctx_read_farfield", "fdtd_dft",
     "fdtd_dft_noalloc",
 )
@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_profile_kernels.argtypes = [v, i, dp]
     L.fdtd_ctx_set_tiling.argtypes = [v, i, i]
     L.fdtd_ctx_get_tiling.argtypes = [v, ip, ip]
+    L.fdtd_ctx_set_prefetch.argtypes = [v, i]
     L.fdtd_ctx_run.argtypes = [v, i]
     L.fdtd_ctx_step.argtypes = [v]
     L.fdtd_status.argtypes = [v, ip, ip]

@@ -17,6 +17,7 @@ from . import _native as N
 CACHE = os.path.join(N.BUILD_DIR, "tiling_cache.json")
 CHUNKS = (1, 2, 4, 8, 16, 32, 64)
 ROWS = (2, 4, 8)
+PREFETCH = (1, 2)
 
 
 def _key(problem, precision: str) -> str:
@@ -38,8 +39,9 @@ def get_tiling(engine) -> tuple[int, int]:
     return a.value, b.value
 
 
-def set_tiling(engine, chunk: int, rows: int) -> None:
+def set_tiling(engine, chunk: int, rows: int, prefetch: int = 1) -> None:
     N.check(N.lib().fdtd_ctx_set_tiling(engine._h, int(chunk), int(rows)))
+    N.check(N.lib().fdtd_ctx_set_prefetch(engine._h, int(prefetch)))
 
 
 def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64, use_cache: bool = True) -> dict:
@@ -49,7 +51,7 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
     cache = _load()
     if use_cache and key in cache:
         return cache[key]
-    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS)) + 8
+    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS) * len(PREFETCH)) + 8
     if problem.grid.numberOfTimeSteps < need:
         raise ValueError(f"the scratch problem needs at least {need} time steps for tuning")
     nx = problem.grid.nx
@@ -60,12 +62,14 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
             if chunk > nx + 1:
                 continue
             for rows in ROWS:
-                set_tiling(eng, chunk, rows)
-                eng.run_timed(steps_per_candidate)          # capture and warm the graph
-                ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
-                table.append({"chunk": chunk, "rows": rows, "ms_per_step": ms})
+                for pf in PREFETCH:
+                    set_tiling(eng, chunk, rows, pf)
+                    eng.run_timed(steps_per_candidate)          # capture and warm the graph
+                    ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
+                    table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "ms_per_step": ms})
     best = min(table, key=lambda r: r["ms_per_step"])
-    out = {"chunk": best["chunk"], "rows": best["rows"], "ms_per_step": best["ms_per_step"], "table": table}
+    out = {"chunk": best["chunk"], "rows": best["rows"], "prefetch": best["prefetch"],
+           "ms_per_step": best["ms_per_step"], "table": table}
     cache[key] = out
     os.makedirs(os.path.dirname(CACHE), exist_ok=True)
     with open(CACHE, "w") as f:
@@ -77,5 +81,5 @@ def apply(engine, precision: str, device: int = 0, scratch_problem=None) -> dict
     """Tunes (on scratch_problem, or the engine's own problem rebuilt with enough
     steps by the caller) and sets the best shape on `engine`."""
     res = tune(scratch_problem or engine.problem, precision, device)
-    set_tiling(engine, res["chunk"], res["rows"])
+    set_tiling(engine, res["chunk"], res["rows"], res.get("prefetch", 1))
     return res

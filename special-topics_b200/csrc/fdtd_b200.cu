@@ -112,7 +112,7 @@ struct fdtd_ctx {
   int* d_ts = nullptr;
   int* d_status = nullptr;
   // launch shape of the step kernels: x planes per thread, thread rows per block
-  int ichunk = 1, block_rows = 8;
+  int ichunk = 1, block_rows = 8, prefetch = 1;
   // graph cache
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -370,11 +370,17 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   const unsigned epi_blocks = (unsigned)((nff + pr.n_v + 255) / 256);
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], c->stream));
-    k_step_h<T, C, EXACT><<<grd, blk, 0, c->stream>>>(p);
+    if (c->prefetch == 2)
+      k_step_h<T, C, EXACT, 2><<<grd, blk, 0, c->stream>>>(p);
+    else
+      k_step_h<T, C, EXACT, 1><<<grd, blk, 0, c->stream>>>(p);
     if (tm) CK(cudaEventRecord(tm->ev[1], c->stream));
     k_step_mid<T, C, EXACT><<<mid_blocks, 256, 0, c->stream>>>(p, pr);
     if (tm) CK(cudaEventRecord(tm->ev[2], c->stream));
-    k_step_e<T, C, EXACT><<<grd, blk, 0, c->stream>>>(p);
+    if (c->prefetch == 2)
+      k_step_e<T, C, EXACT, 2><<<grd, blk, 0, c->stream>>>(p);
+    else
+      k_step_e<T, C, EXACT, 1><<<grd, blk, 0, c->stream>>>(p);
     if (tm) CK(cudaEventRecord(tm->ev[3], c->stream));
     if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, c->stream>>>(p.f, p.g, ff, pr, c->d_ts);
     if (tm) {
@@ -1010,6 +1016,14 @@ int fdtd_ctx_read_material(fdtd_ctx* c, int comp, unsigned char* ids, long n, do
 int fdtd_ctx_run(fdtd_ctx* c, int count) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
   return run_steps(c, count);
+}
+
+int fdtd_ctx_set_prefetch(fdtd_ctx* c, int planes) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (planes != 1 && planes != 2) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in {1,2}", planes);
+  c->prefetch = planes;
+  invalidate(c);
+  return FDTD_OK;
 }
 
 int fdtd_ctx_set_tiling(fdtd_ctx* c, int x_planes_per_thread, int block_rows) {

@@ -327,8 +327,16 @@ __device__ __forceinline__ void h_store(const StepParams<T, C>& p, const HCol<T>
   ey_c = in.ey_n;
 }
 
-template <typename T, class C, bool EXACT>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_h(StepParams<T, C> p) {
+// Minimum resident 256-thread blocks per SM the register budget is fitted to:
+// FP64 values need twice the registers; a deeper prefetch holds one more plane.
+template <typename T, int PF>
+struct MinBlocks {
+  static constexpr int value = sizeof(T) == 8 ? 2 : (PF == 1 ? 4 : 3);
+};
+
+// PF: how many planes ahead the interior loop loads (1 or 2).
+template <typename T, class C, bool EXACT, int PF>
+__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_h(StepParams<T, C> p) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i0 = blockIdx.z * p.ichunk;
@@ -370,12 +378,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_h(StepPara
   for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
   if (xa < xb) {
     // software pipeline: plane i+1's loads are in flight while plane i is computed and stored
-    HIn<T, C> cur, nxt;
+    // software pipeline: the loads of the next PF planes are in flight while
+    // plane i is computed and stored
+    HIn<T, C> cur, nxt, nx2;
     h_load(p, c, xa, cur);
+    if (PF == 2 && xa + 1 < xb) h_load(p, c, xa + 1, nxt);
     for (int i = xa; i < xb; i++) {
-      if (i + 1 < xb) h_load(p, c, i + 1, nxt);
+      if (PF == 1) {
+        if (i + 1 < xb) h_load(p, c, i + 1, nxt);
+      } else {
+        if (i + 2 < xb) h_load(p, c, i + 2, nx2);
+      }
       h_store<T, C, EXACT>(p, c, i, cur, ez_c, ey_c);
       cur = nxt;
+      if (PF == 2) nxt = nx2;
     }
   }
   for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
@@ -560,8 +576,8 @@ __device__ __forceinline__ void e_store(const StepParams<T, C>& p, const ECol<T>
   hy_p = in.hy;
 }
 
-template <typename T, class C, bool EXACT>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_e(StepParams<T, C> p) {
+template <typename T, class C, bool EXACT, int PF>
+__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_e(StepParams<T, C> p) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i0 = blockIdx.z * p.ichunk;
@@ -603,12 +619,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 4) k_step_e(StepPara
   }
   for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
   if (xa < xb) {
-    EIn<T, C> cur, nxt;
+    EIn<T, C> cur, nxt, nx2;
     e_load(p, c, xa, cur);
+    if (PF == 2 && xa + 1 < xb) e_load(p, c, xa + 1, nxt);
     for (int i = xa; i < xb; i++) {
-      if (i + 1 < xb) e_load(p, c, i + 1, nxt);
+      if (PF == 1) {
+        if (i + 1 < xb) e_load(p, c, i + 1, nxt);
+      } else {
+        if (i + 2 < xb) e_load(p, c, i + 2, nx2);
+      }
       e_store<T, C, EXACT>(p, c, i, cur, hz_p, hy_p);
       cur = nxt;
+      if (PF == 2) nxt = nx2;
     }
   }
   for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);

@@ -217,15 +217,15 @@ def test_device_tables_run_matches_host_tables_run():
         assert np.array_equal(a.field("Ez"), b.field("Ez"))
 
 
-@pytest.mark.parametrize("chunk,rows", [(1, 1), (3, 2), (7, 8), (64, 4)])
-def test_launch_shape_does_not_change_fp64_results(chunk, rows):
+@pytest.mark.parametrize("chunk,rows,pf", [(1, 1, 1), (3, 2, 2), (7, 8, 1), (64, 4, 2), (2, 4, 2)])
+def test_launch_shape_does_not_change_fp64_results(chunk, rows, pf):
     from special_topics_b200 import autotune
     scn, steps = CASES["small-zp"]()
     o = oracle.Oracle(scn, steps)
     o.step(steps)
     p = build_problem_from_scenario(scn, steps)
     with Engine(p, "f64") as eng:
-        autotune.set_tiling(eng, min(chunk, p.grid.nx + 1), rows)
+        autotune.set_tiling(eng, min(chunk, p.grid.nx + 1), rows, pf)
         eng.run(steps)
         assert np.array_equal(eng.voltages()[0], o.get("V:0"))
         for fld in ("Hx", "Ey", "Ez"):
@@ -236,7 +236,7 @@ def test_autotuner_picks_a_measured_shape(tmp_path, monkeypatch):
     from special_topics_b200 import autotune
     monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tiling.json"))
     scn, _ = CASES["small-xp"]()
-    p = build_problem_from_scenario(scn, 400)
+    p = build_problem_from_scenario(scn, 800)
     res = autotune.tune(p, "f32-table", steps_per_candidate=8)
     assert {"chunk", "rows", "ms_per_step"} <= set(res)
     assert res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
