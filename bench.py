@@ -179,6 +179,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
+    ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
@@ -225,6 +227,15 @@ def main():
     from special_topics_b200 import workloads
     from special_topics_b200.backend import Engine
     from special_topics_b200.scenario import build_problem_from_scenario
+
+    # batched-sweep members are built on host processes started before any GPU work
+    variants = None
+    if rank == 0 and world == 1 and args.batch_members > 0:
+        import multiprocessing as mp
+        from special_topics_b200 import autotune as _at
+        vsteps = 2 * args.warmup + args.batch_steps + 16 + _at.batch_steps_needed(args.tune_steps)
+        with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+            variants = variant_problems(args.batch_members, max(7000, vsteps), pool)
 
     K, W, P = args.steps, args.warmup, 16
     scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P)
@@ -299,6 +310,9 @@ def main():
         "e2e": e2e,
         "setup_s": setup_s,
     }
+    if variants:
+        line["batched"] = batched_side(variants, K=args.batch_steps, W=args.warmup, tune_steps=args.tune_steps,
+                                       device=local)
     if rank == 0 and world == 1 and not args.no_fp64:
         line["fp64_plain"] = fp64_side(pkg)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -324,6 +338,64 @@ def _uploaded_bytes(p, precision: str) -> int:
     for vs in p.voltage_sources:
         b += vs.field_indices.nbytes + vs.coef.nbytes + vs.voltage_per_e_field.nbytes
     return b
+
+
+def _variant_problem(args):
+    seed, steps = args
+    pkg = _package()
+    from special_topics_b200 import workloads
+    from special_topics_b200.scenario import build_problem_from_scenario
+    return build_problem_from_scenario(workloads.ifa_variant(seed, steps=steps), steps, per_cell=False)
+
+
+def variant_problems(count: int, steps: int, pool=None) -> list:
+    """The batched-sweep members (inverted-F variants, seeds 0..count-1)."""
+    _package()    # results unpickle into the package's classes
+    jobs = [(s, steps) for s in range(count)]
+    if pool is None:
+        return [_variant_problem(j) for j in jobs]
+    return pool.map(_variant_problem, jobs)
+
+
+def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, device: int = 0) -> dict:
+    """The batched sweep: every member advanced by one set of four launches per
+    step (FP32 fields, material tables), launch shape from the batch autotuner."""
+    from special_topics_b200 import autotune
+    from special_topics_b200.backend import Batch, Engine
+    t0 = time.perf_counter()
+    engs = [Engine(p, "f32-table", device=device) for p in problems]
+    create_s = time.perf_counter() - t0
+    try:
+        with Batch(engs) as b:
+            tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
+            b.run(W)
+            with ClockSampler(device) as clk:
+                ms = b.run_timed(K)
+            kern = b.profile_kernels(8)
+            cells = b.cells
+            tiling = b.tiling()
+    finally:
+        for e in engs:
+            e.close()
+    byts = {"h": 0, "e": 0}
+    for p in problems:
+        a = algorithmic_bytes(p, "f32-table")
+        byts["h"] += a["h"]
+        byts["e"] += a["e"]
+    dom = "e" if kern["e"] >= kern["h"] else "h"
+    peak, peak_kind = hbm_peak()
+    ach = byts[dom] / (kern[dom] / 1e3) / 1e9
+    dims = [(p.grid.nx, p.grid.ny, p.grid.nz) for p in problems]
+    return {"workload": f"ifa-variants-{len(problems)}", "members": len(problems), "cells": cells,
+            "grid_min": list(min(dims, key=lambda d: d[0] * d[1] * d[2])),
+            "grid_max": list(max(dims, key=lambda d: d[0] * d[1] * d[2])),
+            "value": cells * K / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "gpu_launches": 4 * K, "kernel_ms": kern,
+            "tiling": tiling, "tuning_ms_per_step": tuning["ms_per_step"],
+            "roofline": {"bound": "hbm", "kernel": f"k_batch_half ({dom.upper()})", "achieved": ach, "peak": peak,
+                         "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom]},
+            "clocks": clk.summary(), "engine_create_s": create_s}
 
 
 def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:

@@ -193,6 +193,35 @@ int fdtd_ctx_step(const fdtd_ctx* ctx);
 /* Watchdog: *code = FDTD_OK or FDTD_ERR_NONFINITE, *step = first bad step or -1. */
 int fdtd_status(fdtd_ctx* ctx, int* code, int* step);
 
+/* ---- batches: many handles advanced together (no counterpart in the reference,
+ * which runs one problem per process through its global context,
+ * fdtd_cuda.cu:44-118; the batched sweep is SURVEY's configuration 3) ---- */
+typedef struct fdtd_batch fdtd_batch;
+
+/* Groups `count` handles of one device and one precision.  The batch owns no
+ * member: members stay valid handles (readbacks, fdtd_status, their own runs)
+ * and must outlive the batch.  Each step of fdtd_batch_run is four launches for
+ * the whole batch: H over a tile list spanning every member, the mid-step
+ * kernel, E over the tile list, and the far-field/port epilogue. */
+int fdtd_batch_create(fdtd_ctx* const* members, int count, fdtd_batch** out);
+void fdtd_batch_free(fdtd_batch* batch);
+int fdtd_batch_size(const fdtd_batch* batch);
+/* Launch shape shared by all members: x planes per thread and block rows as in
+ * fdtd_ctx_set_tiling, prefetch depth as in fdtd_ctx_set_prefetch, and `group`:
+ * 0 = one block per tile; g > 0 = a persistent grid (as many blocks as are
+ * resident on the device) whose blocks claim g consecutive tiles at a time from
+ * a device counter.  Results do not depend on the shape. */
+int fdtd_batch_set_tiling(fdtd_batch* batch, int x_planes_per_thread, int block_rows, int prefetch, int group);
+int fdtd_batch_get_tiling(const fdtd_batch* batch, int* x_planes_per_thread, int* block_rows, int* prefetch,
+                          int* group);
+/* Runs `count` steps of every member.  All members must be at the same step and
+ * have `count` steps left.  Returns FDTD_ERR_NONFINITE naming the first member
+ * whose watchdog fired. */
+int fdtd_batch_run(fdtd_batch* batch, int count);
+int fdtd_batch_run_timed(fdtd_batch* batch, int count, float* ms);
+/* Per-kernel mean durations (ms) of the batch's H, mid-step, E and epilogue launches. */
+int fdtd_batch_profile_kernels(fdtd_batch* batch, int count, double* avg_ms);
+
 /* Whole probe traces, FP64, one value per step (first `n` steps). kind 0 = voltage, 1 = current. */
 int fdtd_ctx_read_trace(fdtd_ctx* ctx, int kind, int probe, double* out, int n);
 /* Field `which` as FP64 (FP32 problems are widened). */

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(PKG_DIR)
 BUILD_DIR = os.path.join(PKG_DIR, "_build")
 LIB_PATH = os.path.join(BUILD_DIR, "libfdtd_b200.so")
 SOURCES = [os.path.join(PKG_DIR, "csrc", f) for f in
-           ("fdtd_b200.cu", "fdtd_common.cuh", "fdtd_step.cuh", "fdtd_material.cuh")]
+           ("fdtd_b200.cu", "fdtd_common.cuh", "fdtd_step.cuh", "fdtd_material.cuh", "fdtd_batch.cuh")]
 HEADER = os.path.join(ROOT, "include", "fdtd_b200.h")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -32,7 +32,8 @@ EXPORTS = (
     "fdtd_ctx_override_material", "fdtd_ctx_read_material", "fdtd_ctx_run", "fdtd_ctx_run_timed",
     "fdtd_ctx_profile_kernels", "fdtd_ctx_set_tiling", "fdtd_ctx_get_tiling", "fdtd_ctx_set_prefetch", "fdtd_ctx_step", "fdtd_status",
     "fdtd_ctx_read_trace", "fdtd_ctx_read_field", "fdtd_ctx_read_psi", "fdtd_ctx_read_farfield", "fdtd_dft",
-    "fdtd_dft_noalloc",
+    "fdtd_dft_noalloc", "fdtd_batch_create", "fdtd_batch_free", "fdtd_batch_size", "fdtd_batch_set_tiling",
+    "fdtd_batch_get_tiling", "fdtd_batch_run", "fdtd_batch_run_timed", "fdtd_batch_profile_kernels",
 )
 
 
@@ -117,6 +118,15 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_read_farfield.argtypes = [v, i, dp, dp, lp]
     L.fdtd_dft.argtypes = [dp, i, d, dp, i, d, dp, dp]
     L.fdtd_dft_noalloc.argtypes = [dp, i, d, dp, i, d, dp, dp]
+    L.fdtd_batch_create.argtypes = [P(v), i, P(v)]
+    L.fdtd_batch_free.argtypes = [v]
+    L.fdtd_batch_free.restype = None
+    L.fdtd_batch_size.argtypes = [v]
+    L.fdtd_batch_set_tiling.argtypes = [v, i, i, i, i]
+    L.fdtd_batch_get_tiling.argtypes = [v, ip, ip, ip, ip]
+    L.fdtd_batch_run.argtypes = [v, i]
+    L.fdtd_batch_run_timed.argtypes = [v, i, fp]
+    L.fdtd_batch_profile_kernels.argtypes = [v, i, dp]
     L.fdtd_init.argtypes = [P(FdtdDims)]
     L.fdtd_upload_coeff.argtypes = [i, fp, i]
     L.fdtd_upload_cpml.argtypes = [i, i, fp, fp, fp, fp, fp, i, fp, i, fp, i, fp, i, i, i, i]

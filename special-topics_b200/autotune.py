@@ -77,6 +77,61 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
     return out
 
 
+BATCH_CHUNKS = (2, 4, 8, 16, 32)
+BATCH_GROUPS = (0, 1, 2, 4, 8, 16)
+
+
+def batch_key(batch) -> str:
+    """Grid class of a batch: precision, member count and the member grid
+    extents rounded up to multiples of 16 cells."""
+    dims = sorted(tuple(-(-d // 16) * 16 for d in (e.problem.grid.nx, e.problem.grid.ny, e.problem.grid.nz))
+                  for e in batch.engines)
+    lo, hi = dims[0], dims[-1]
+    return f"batch:{batch.engines[0].precision}:{len(dims)}:{lo[0]}x{lo[1]}x{lo[2]}-{hi[0]}x{hi[1]}x{hi[2]}"
+
+
+def batch_steps_needed(steps_per_candidate: int) -> int:
+    return 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(PREFETCH) + len(BATCH_GROUPS))
+
+
+def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> dict:
+    """Tunes a batch's shared launch shape on the batch itself (every shape
+    computes the same values, so tuning only advances the members by
+    batch_steps_needed(steps_per_candidate) steps).  First x planes per thread,
+    block rows and prefetch depth with one block per tile, then the tile group
+    of the persistent grid at that shape.  Sets and returns the fastest."""
+    key = batch_key(batch)
+    cache = _load()
+    if use_cache and key in cache:
+        r = cache[key]
+        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"])
+        return r
+    max_x = max(e.problem.grid.nx for e in batch.engines) + 1
+    table = []
+
+    def trial(chunk, rows, pf, group):
+        batch.set_tiling(chunk, rows, pf, group)
+        batch.run_timed(steps_per_candidate)              # capture and warm the graph
+        ms = batch.run_timed(steps_per_candidate) / steps_per_candidate
+        table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "ms_per_step": ms})
+
+    for chunk in BATCH_CHUNKS:
+        for rows in ROWS:
+            for pf in PREFETCH:
+                trial(min(chunk, max_x), rows, pf, 0)
+    best = min(table, key=lambda r: r["ms_per_step"])
+    for group in BATCH_GROUPS[1:]:
+        trial(best["chunk"], best["rows"], best["prefetch"], group)
+    best = min(table, key=lambda r: r["ms_per_step"])
+    out = dict(best, table=table)
+    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"])
+    cache[key] = out
+    os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+    with open(CACHE, "w") as f:
+        json.dump(cache, f, indent=1)
+    return out
+
+
 def apply(engine, precision: str, device: int = 0, scratch_problem=None) -> dict:
     """Tunes (on scratch_problem, or the engine's own problem rebuilt with enough
     steps by the caller) and sets the best shape on `engine`."""

@@ -203,6 +203,69 @@ class Engine:
             pass
 
 
+class Batch:
+    """Engines of one precision on one device advanced together: every step is
+    four launches for the whole batch (fdtd_batch_* in include/fdtd_b200.h).
+    The engines stay usable for readback and must outlive the batch."""
+
+    def __init__(self, engines: list, chunk: int = 8, rows: int = 4, prefetch: int = 1, group: int = 0):
+        if not engines:
+            raise ValueError("a batch needs at least one engine")
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h.value for e in self.engines])
+        h = C.c_void_p()
+        N.check(N.lib().fdtd_batch_create(arr, len(self.engines), C.byref(h)))
+        self._h = h
+        self.set_tiling(chunk, rows, prefetch, group)
+
+    def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0) -> None:
+        N.check(N.lib().fdtd_batch_set_tiling(self._h, int(chunk), int(rows), int(prefetch), int(group)))
+
+    def tiling(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        N.check(N.lib().fdtd_batch_get_tiling(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("chunk", "rows", "prefetch", "group"), [x.value for x in v]))
+
+    @property
+    def cells(self) -> int:
+        return sum(e.problem.grid.nx * e.problem.grid.ny * e.problem.grid.nz for e in self.engines)
+
+    @property
+    def step(self) -> int:
+        return self.engines[0].step
+
+    def run(self, count: int) -> None:
+        N.check(N.lib().fdtd_batch_run(self._h, int(count)))
+
+    def run_timed(self, count: int) -> float:
+        ms = C.c_float()
+        N.check(N.lib().fdtd_batch_run_timed(self._h, int(count), C.byref(ms)))
+        return ms.value
+
+    def profile_kernels(self, count: int) -> dict:
+        out = np.zeros(4)
+        N.check(N.lib().fdtd_batch_profile_kernels(self._h, int(count), N.dptr(out)))
+        return dict(zip(("h", "mid", "e", "epilogue"), out.tolist()))
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.lib().fdtd_batch_free(h)
+        self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class B200Backend:
     """Backend object of the reference's registry contract (CONTRACT.md:121-137)."""
 

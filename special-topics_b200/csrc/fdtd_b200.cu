@@ -16,6 +16,7 @@
 #include "fdtd_common.cuh"
 #include "fdtd_material.cuh"
 #include "fdtd_step.cuh"
+#include "fdtd_batch.cuh"
 
 #include <map>
 #include <mutex>
@@ -1220,6 +1221,348 @@ int fdtd_dft_noalloc(const double* x, int N, double dt, const double* freqs, int
   CK(cudaMemcpy(im, d_im, M * sizeof(double), cudaMemcpyDeviceToHost));
   return FDTD_OK;
 }
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches: member handles advanced together, one launch per kernel kind per
+// step for all of them (fdtd_batch.cuh).
+// ===========================================================================
+struct fdtd_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int prec = FDTD_PREC_F32_TABLE;
+  std::vector<fdtd_ctx*> m;
+  int ichunk = 8, block_rows = 4, prefetch = 1, group = 0;
+  void* d_inst = nullptr;
+  size_t inst_size = 0;  // bytes of one Instance
+  BatchTile* d_tiles = nullptr;
+  BatchBlock* d_mid = nullptr;
+  BatchBlock* d_epi = nullptr;
+  BatchCtl* d_ctl = nullptr;
+  std::vector<BatchTile> tiles;
+  std::vector<BatchBlock> mid, epi;
+  int grid_h = 0, grid_e = 0;  // persistent grid sizes
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+void batch_drop_graph(fdtd_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+template <class V>
+int upload_vec(fdtd_batch* b, V** dst, const std::vector<V>& v) {
+  if (*dst) cudaFree(*dst);
+  *dst = nullptr;
+  const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(V);
+  CK(cudaMalloc((void**)dst, bytes));
+  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return FDTD_OK;
+}
+
+// The parameter blocks of every member (member state may have moved since the
+// last run: traces, tables) and, when the work lists changed, the lists.
+template <typename T, class C, bool EXACT>
+int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
+  using In = Instance<T, C>;
+  const int n = (int)b->m.size();
+  std::vector<unsigned char> host((size_t)n * sizeof(In), 0);
+  std::vector<BatchTile> tiles;
+  std::vector<BatchBlock> mid, epi;
+  for (int q = 0; q < n; q++) {
+    fdtd_ctx* c = b->m[q];
+    In in;
+    memset(&in, 0, sizeof(In));
+    in.sp = step_params<T, C>(c, coef_of(c));
+    in.sp.ichunk = b->ichunk;
+    in.sp.ts = &b->d_ctl->ts;
+    in.pr = dev_probes(c);
+    in.ff = dev_ff(c);
+    memcpy(host.data() + (size_t)q * sizeof(In), &in, sizeof(In));
+    const int gx = (c->nz + 1 + 31) / 32, gy = (c->ny + b->block_rows) / b->block_rows,
+              gz = (c->nx + 1 + b->ichunk - 1) / b->ichunk;
+    if (gx > 65535 || gy > 65535 || gz > 65535)
+      return fail(FDTD_ERR_BADARG, "batch member %d: %dx%dx%d tiles exceed the tile index range", q, gx, gy, gz);
+    for (int z = 0; z < gz; z++)
+      for (int y = 0; y < gy; y++)
+        for (int x = 0; x < gx; x++)
+          tiles.push_back(BatchTile{(unsigned short)q, (unsigned short)x, (unsigned short)y, (unsigned short)z});
+    const long long nmid = (long long)c->ny * (c->nz + 1) + in.pr.n_i;
+    for (long long s = 0; s < (nmid + 255) / 256; s++) mid.push_back(BatchBlock{q, (int)s});
+    const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
+    for (long long s = 0; s < (nff + in.pr.n_v + 255) / 256; s++) epi.push_back(BatchBlock{q, (int)s});
+  }
+  if (tiles.size() > (size_t)INT32_MAX) return fail(FDTD_ERR_BADARG, "batch has too many tiles");
+  if (!b->d_inst || b->inst_size != sizeof(In)) {
+    if (b->d_inst) cudaFree(b->d_inst);
+    b->d_inst = nullptr;
+    CK(cudaMalloc(&b->d_inst, host.size()));
+    b->inst_size = sizeof(In);
+  }
+  CK(cudaMemcpyAsync(b->d_inst, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  auto same = [](const std::vector<BatchBlock>& u, const std::vector<BatchBlock>& v) {
+    return u.size() == v.size() && (u.empty() || !memcmp(u.data(), v.data(), u.size() * sizeof(BatchBlock)));
+  };
+  const bool same_tiles = tiles.size() == b->tiles.size() &&
+                          (tiles.empty() || !memcmp(tiles.data(), b->tiles.data(), tiles.size() * sizeof(BatchTile)));
+  if (!same_tiles || !same(mid, b->mid) || !same(epi, b->epi) || !b->d_tiles) {
+    batch_drop_graph(b);
+    b->tiles.swap(tiles);
+    b->mid.swap(mid);
+    b->epi.swap(epi);
+    int rc = upload_vec(b, &b->d_tiles, b->tiles);
+    if (!rc) rc = upload_vec(b, &b->d_mid, b->mid);
+    if (!rc) rc = upload_vec(b, &b->d_epi, b->epi);
+    if (rc) return rc;
+  }
+  // persistent grids: as many blocks as fit on the device at once
+  int sms = 0, per_h = 0, per_e = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  const int threads = 32 * b->block_rows;
+  if (b->prefetch == 2) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_h, k_batch_half<T, C, EXACT, 2, false, true>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_e, k_batch_half<T, C, EXACT, 2, true, true>, threads, 0));
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_h, k_batch_half<T, C, EXACT, 1, false, true>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_e, k_batch_half<T, C, EXACT, 1, true, true>, threads, 0));
+  }
+  b->grid_h = std::max(1, per_h) * sms;
+  b->grid_e = std::max(1, per_e) * sms;
+  return FDTD_OK;
+}
+
+template <typename T, class C, bool EXACT>
+int batch_enqueue(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
+  const Instance<T, C>* in = (const Instance<T, C>*)b->d_inst;
+  const int nt = (int)b->tiles.size();
+  const dim3 blk(32, b->block_rows);
+  const unsigned gh = b->group ? (unsigned)std::min(b->grid_h, (nt + b->group - 1) / b->group) : (unsigned)nt;
+  const unsigned ge = b->group ? (unsigned)std::min(b->grid_e, (nt + b->group - 1) / b->group) : (unsigned)nt;
+  // kernel for (prefetch, electric, persistent)
+  using K = void (*)(const Instance<T, C>*, const BatchTile*, int, BatchCtl*, int);
+  const K kern[2][2][2] = {{{k_batch_half<T, C, EXACT, 1, false, false>, k_batch_half<T, C, EXACT, 1, false, true>},
+                            {k_batch_half<T, C, EXACT, 1, true, false>, k_batch_half<T, C, EXACT, 1, true, true>}},
+                           {{k_batch_half<T, C, EXACT, 2, false, false>, k_batch_half<T, C, EXACT, 2, false, true>},
+                            {k_batch_half<T, C, EXACT, 2, true, false>, k_batch_half<T, C, EXACT, 2, true, true>}}};
+  const int pf = b->prefetch == 2 ? 1 : 0, ps = b->group ? 1 : 0;
+  for (int s = 0; s < count; s++) {
+    if (tm) CK(cudaEventRecord(tm->ev[0], b->stream));
+    kern[pf][0][ps]<<<gh, blk, 0, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    if (tm) CK(cudaEventRecord(tm->ev[1], b->stream));
+    k_batch_mid<T, C, EXACT><<<(unsigned)b->mid.size(), 256, 0, b->stream>>>(in, b->d_mid, b->d_ctl);
+    if (tm) CK(cudaEventRecord(tm->ev[2], b->stream));
+    kern[pf][1][ps]<<<ge, blk, 0, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    if (tm) CK(cudaEventRecord(tm->ev[3], b->stream));
+    if (!b->epi.empty()) k_batch_epilogue<T, C><<<(unsigned)b->epi.size(), 256, 0, b->stream>>>(in, b->d_epi);
+    if (tm) {
+      CK(cudaEventRecord(tm->ev[4], b->stream));
+      CK(cudaEventSynchronize(tm->ev[4]));
+      for (int q = 0; q < 4; q++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, tm->ev[q], tm->ev[q + 1]));
+        tm->ms[q] += ms;
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+ArrayCoef<double> coef_f64(fdtd_ctx* c) { return array_coef<double>(c); }
+ArrayCoef<float> coef_f32(fdtd_ctx* c) { return array_coef<float>(c); }
+TableCoef coef_table(fdtd_ctx* c) { return c->tcoef; }
+
+int batch_prepare_any(fdtd_batch* b) {
+  if (b->prec == FDTD_PREC_F64) return batch_prepare<double, ArrayCoef<double>, true>(b, coef_f64);
+  if (b->prec == FDTD_PREC_F32) return batch_prepare<float, ArrayCoef<float>, true>(b, coef_f32);
+  return batch_prepare<float, TableCoef, false>(b, coef_table);
+}
+
+int batch_enqueue_any(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
+  if (b->prec == FDTD_PREC_F64) return batch_enqueue<double, ArrayCoef<double>, true>(b, count, tm);
+  if (b->prec == FDTD_PREC_F32) return batch_enqueue<float, ArrayCoef<float>, true>(b, count, tm);
+  return batch_enqueue<float, TableCoef, false>(b, count, tm);
+}
+
+int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer* tm = nullptr) {
+  if (count < 0) return fail(FDTD_ERR_BADARG, "negative step count %d", count);
+  const int ts = b->m[0]->ts;
+  for (size_t q = 0; q < b->m.size(); q++) {
+    fdtd_ctx* c = b->m[q];
+    if (c->ts != ts) return fail(FDTD_ERR_STATE, "batch member %zu is at step %d, member 0 at step %d", q, c->ts, ts);
+    if (ts + count > c->nsteps)
+      return fail(FDTD_ERR_BADARG, "batch member %zu: running %d steps from step %d exceeds numberOfTimeSteps=%d", q,
+                  count, ts, c->nsteps);
+    int rc = check_ready(c);
+    if (!rc) rc = ensure_traces(c);
+    if (!rc && c->prec == FDTD_PREC_F32_TABLE && c->table_dirty) rc = prepare_table(c, &c->tcoef);
+    if (rc) {
+      std::string msg = g_err;
+      return fail(rc, "batch member %zu: %s", q, msg.c_str());
+    }
+  }
+  CK(cudaSetDevice(b->device));
+  int rc = batch_prepare_any(b);
+  if (rc) return rc;
+  const int ctl_ts = ts - 1;
+  CK(cudaMemcpyAsync(&b->d_ctl->ts, &ctl_ts, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (elapsed_ms) {
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, b->stream));
+  }
+  int left = count;
+  if (tm) {
+    rc = batch_enqueue_any(b, left, tm);
+    if (rc) return rc;
+    left = 0;
+  }
+  while (left >= kGraphSteps) {
+    if (!b->graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int erc = batch_enqueue_any(b, kGraphSteps);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      if (erc) return erc;
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    CK(cudaGraphLaunch(b->graph, b->stream));
+    left -= kGraphSteps;
+  }
+  if (left > 0) {
+    rc = batch_enqueue_any(b, left);
+    if (rc) return rc;
+  }
+  if (elapsed_ms) {
+    CK(cudaEventRecord(ev1, b->stream));
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  // hand the shared step counter back to every member
+  for (fdtd_ctx* c : b->m) CK(cudaMemcpyAsync(c->d_ts, &b->d_ctl->ts, sizeof(int), cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (fdtd_ctx* c : b->m) c->ts += count;
+  for (size_t q = 0; q < b->m.size(); q++) {
+    int st[2];
+    CK(cudaMemcpyAsync(st, b->m[q]->d_status, sizeof(st), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    if (st[0] != 0) return fail(FDTD_ERR_NONFINITE, "batch member %zu: non-finite port sample at step %d", q, st[1]);
+  }
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(fdtd_ctx* const* members, int count, fdtd_batch** out) {
+  if (!members || !out || count < 1) return fail(FDTD_ERR_BADARG, "bad batch arguments");
+  *out = nullptr;
+  if (count > 65535) return fail(FDTD_ERR_BADARG, "a batch holds at most 65535 members");
+  for (int q = 0; q < count; q++) {
+    if (!members[q]) return fail(FDTD_ERR_BADARG, "batch member %d is NULL", q);
+    if (members[q]->device != members[0]->device || members[q]->prec != members[0]->prec)
+      return fail(FDTD_ERR_BADARG, "batch member %d differs from member 0 in device or precision", q);
+    for (int r = 0; r < q; r++)
+      if (members[r] == members[q]) return fail(FDTD_ERR_BADARG, "batch member %d repeats member %d", q, r);
+  }
+  fdtd_batch* b = new fdtd_batch();
+  b->device = members[0]->device;
+  b->prec = members[0]->prec;
+  b->m.assign(members, members + count);
+  if (cudaSetDevice(b->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return fail(FDTD_ERR_CUDA, "cannot create a stream on device %d", members[0]->device);
+  }
+  BatchCtl zero{};
+  if (cudaMalloc((void**)&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+      cudaMemcpyAsync(b->d_ctl, &zero, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess) {
+    fdtd_batch_free(b);
+    return fail(FDTD_ERR_CUDA, "cannot allocate the batch control block");
+  }
+  *out = b;
+  return FDTD_OK;
+}
+
+void fdtd_batch_free(fdtd_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  cudaFree(b->d_inst);
+  cudaFree(b->d_tiles);
+  cudaFree(b->d_mid);
+  cudaFree(b->d_epi);
+  cudaFree(b->d_ctl);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int fdtd_batch_set_tiling(fdtd_batch* b, int x_planes_per_thread, int block_rows, int prefetch, int group) {
+  if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
+  if (x_planes_per_thread < 1 || x_planes_per_thread > 1024)
+    return fail(FDTD_ERR_BADARG, "x planes per thread %d outside 1..1024", x_planes_per_thread);
+  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8)
+    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8}", block_rows);
+  if (prefetch != 1 && prefetch != 2) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in {1,2}", prefetch);
+  if (group < 0 || group > 4096) return fail(FDTD_ERR_BADARG, "tile group %d outside 0..4096", group);
+  if (b->ichunk != x_planes_per_thread || b->block_rows != block_rows || b->prefetch != prefetch ||
+      b->group != group)
+    batch_drop_graph(b);
+  b->ichunk = x_planes_per_thread;
+  b->block_rows = block_rows;
+  b->prefetch = prefetch;
+  b->group = group;
+  return FDTD_OK;
+}
+
+int fdtd_batch_get_tiling(const fdtd_batch* b, int* x_planes_per_thread, int* block_rows, int* prefetch,
+                          int* group) {
+  if (!b || !x_planes_per_thread || !block_rows || !prefetch || !group) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *x_planes_per_thread = b->ichunk;
+  *block_rows = b->block_rows;
+  *prefetch = b->prefetch;
+  *group = b->group;
+  return FDTD_OK;
+}
+
+int fdtd_batch_run(fdtd_batch* b, int count) {
+  if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
+  return batch_run(b, count);
+}
+
+int fdtd_batch_run_timed(fdtd_batch* b, int count, float* ms) {
+  if (!b || !ms) return fail(FDTD_ERR_BADARG, "NULL argument");
+  return batch_run(b, count, ms);
+}
+
+int fdtd_batch_profile_kernels(fdtd_batch* b, int count, double* avg_ms) {
+  if (!b || !avg_ms || count < 1) return fail(FDTD_ERR_BADARG, "bad arguments");
+  KernelTimer tm;
+  CK(cudaSetDevice(b->device));
+  for (int q = 0; q < 5; q++) CK(cudaEventCreate(&tm.ev[q]));
+  int rc = batch_run(b, count, nullptr, &tm);
+  for (int q = 0; q < 5; q++) cudaEventDestroy(tm.ev[q]);
+  if (rc) return rc;
+  for (int q = 0; q < 4; q++) avg_ms[q] = tm.ms[q] / count;
+  return FDTD_OK;
+}
+
+int fdtd_batch_size(const fdtd_batch* b) { return b ? (int)b->m.size() : -1; }
 
 // ===========================================================================
 // Legacy global-context API (fdtd_cuda.h), FP32 per-cell coefficients.

@@ -142,10 +142,9 @@ __device__ __forceinline__ void acc2(const FarField& ff, int a, long long p, dou
 // pairs share the point), looping over frequencies.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_epilogue(Fields<T> f, GridDims g, FarField ff, Probes probes,
-                                                  const int* ts_ptr) {
+__device__ __forceinline__ void epilogue_thread(const Fields<T>& f, const GridDims& g, const FarField& ff,
+                                                const Probes& probes, const int* ts_ptr, long long t) {
   const int ts = *ts_ptr;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int ny = g.ny, nz = g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const long long nff = ff.nFreq > 0 ? ff.sz[0] + ff.sz[1] + ff.sz[2] : 0;
   if (t >= nff) {
@@ -247,6 +246,12 @@ __global__ void __launch_bounds__(256) k_epilogue(Fields<T> f, GridDims g, FarFi
 #undef EX
 #undef EY
 #undef EZ
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_epilogue(Fields<T> f, GridDims g, FarField ff, Probes probes,
+                                                  const int* ts_ptr) {
+  epilogue_thread<T>(f, g, ff, probes, ts_ptr, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace fdtd

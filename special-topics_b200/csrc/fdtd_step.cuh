@@ -334,14 +334,13 @@ struct MinBlocks {
   static constexpr int value = sizeof(T) == 8 ? 2 : (PF == 1 ? 4 : 3);
 };
 
-// PF: how many planes ahead the interior loop loads (1 or 2).
+// H update of one tile: columns (bx*32 + tx, by*rows + ty), x planes from
+// bz*ichunk.  PF: how many planes ahead the interior loop loads (1 or 2).
 template <typename T, class C, bool EXACT, int PF>
-__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_h(StepParams<T, C> p) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i0 = blockIdx.z * p.ichunk;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
-    *p.ts += 1;  // first kernel of a step advances the device step counter
+__device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
+  const int k = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int i0 = bz * p.ichunk;
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
   const bool valid = j <= ny && k <= nz;
   HCol<T> c;
@@ -397,15 +396,21 @@ __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_h(StepPar
   for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
 }
 
+template <typename T, class C, bool EXACT, int PF>
+__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_h(StepParams<T, C> p) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+    *p.ts += 1;  // first kernel of a step advances the device step counter
+  step_h_tile<T, C, EXACT, PF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // ---------------------------------------------------------------------------
 // Mid-step: the bulk-updated Ex(i=0) plane and the port currents.
 // ---------------------------------------------------------------------------
 template <typename T, class C, bool EXACT>
-__global__ void __launch_bounds__(256) k_step_mid(StepParams<T, C> p, Probes probes) {
+__device__ __forceinline__ void step_mid_thread(const StepParams<T, C>& p, const Probes& probes, long long t) {
   using A = Ar<T, EXACT>;
   const int ts = *p.ts;
   const int ny = p.g.ny, nz = p.g.nz, nzp1 = nz + 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long plane = (long long)ny * nzp1;
   if (t < plane) {
     const int j = (int)(t / nzp1), k = (int)(t % nzp1);
@@ -422,6 +427,11 @@ __global__ void __launch_bounds__(256) k_step_mid(StepParams<T, C> p, Probes pro
   } else if (t - plane < probes.n_i) {
     current_probe(p.f, probes, (int)(t - plane), ts);
   }
+}
+
+template <typename T, class C, bool EXACT>
+__global__ void __launch_bounds__(256) k_step_mid(StepParams<T, C> p, Probes probes) {
+  step_mid_thread<T, C, EXACT>(p, probes, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -577,10 +587,10 @@ __device__ __forceinline__ void e_store(const StepParams<T, C>& p, const ECol<T>
 }
 
 template <typename T, class C, bool EXACT, int PF>
-__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_e(StepParams<T, C> p) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i0 = blockIdx.z * p.ichunk;
+__device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
+  const int k = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int i0 = bz * p.ichunk;
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
   const bool valid = j <= ny && k <= nz;
   ECol<T> c;
@@ -634,6 +644,11 @@ __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_e(StepPar
     }
   }
   for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+}
+
+template <typename T, class C, bool EXACT, int PF>
+__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_e(StepParams<T, C> p) {
+  step_e_tile<T, C, EXACT, PF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace fdtd

@@ -1,0 +1,165 @@
+"""Batched runs: members of uneven size advanced together give exactly what
+each member gives when run on its own (same kernels, same arithmetic per
+cell), for every launch shape, including the persistent tile-claiming grid."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import load_package, load_scenario
+from scenarios_small import small_scenario
+
+pkg = load_package()
+from special_topics_b200 import _native as N  # noqa: E402
+from special_topics_b200.backend import Batch, Engine  # noqa: E402
+from special_topics_b200.scenario import FF_NAMES, build_problem_from_scenario  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 70   # one 64-step graph replay plus 6 single steps
+
+
+def _members(steps=STEPS):
+    scns = [small_scenario(1, "xp"), small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3)),
+            small_scenario(3, "zp", ncpml=(5, 4, 3, 3, 4, 5)), load_scenario("ifa-fr4-substrate")]
+    return [build_problem_from_scenario(s, steps) for s in scns]
+
+
+def _state(eng):
+    out = {"V": eng.voltages(), "I": eng.currents()}
+    for f in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"):
+        out[f] = eng.field(f)
+    ff = eng.farfield()
+    for a in FF_NAMES:
+        out[a] = ff[a]
+    return out
+
+
+def _assert_same(a, b, tag):
+    for key in a:
+        x, y = a[key], b[key]
+        if isinstance(x, (list, tuple)):
+            for q, (u, v) in enumerate(zip(x, y)):
+                assert np.array_equal(u, v), f"{tag} {key}[{q}]"
+        else:
+            assert np.array_equal(x, y), f"{tag} {key}"
+
+
+@pytest.fixture(scope="module", params=["f64", "f32-table"])
+def solo(request):
+    probs = _members()
+    states = []
+    for p in probs:
+        with Engine(p, request.param) as eng:
+            eng.run(STEPS)
+            states.append(_state(eng))
+    return request.param, states
+
+
+@pytest.mark.parametrize("chunk,rows,pf,group", [(8, 4, 1, 0), (3, 2, 2, 0), (1, 8, 1, 1), (5, 4, 1, 7),
+                                                 (16, 2, 2, 3)])
+def test_batch_matches_solo_runs(solo, chunk, rows, pf, group):
+    precision, states = solo
+    engs = [Engine(p, precision) for p in _members()]
+    try:
+        with Batch(engs, chunk, rows, pf, group) as b:
+            assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group}
+            b.run(STEPS)
+            assert b.step == STEPS
+        for q, e in enumerate(engs):
+            assert e.step == STEPS
+            assert e.status() == (0, -1)
+            _assert_same(states[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_batch_fp64_matches_oracle():
+    scn = small_scenario(5, "yn", ncpml=(3, 4, 5, 6, 3, 4))
+    o = oracle.Oracle(scn, 40)
+    o.step(40)
+    probs = [build_problem_from_scenario(scn, 40), build_problem_from_scenario(small_scenario(6, "zp"), 40)]
+    engs = [Engine(p, "f64") for p in probs]
+    try:
+        with Batch(engs, 4, 4, 1, 2) as b:
+            b.run(25)
+            b.run(15)    # a second run resumes from the members' step
+        assert np.array_equal(engs[0].voltages()[0], o.get("V:0"))
+        assert np.array_equal(engs[0].currents()[0], o.get("I:0"))
+        assert np.array_equal(engs[0].field("Ez"), o.get("Ez"))
+        # members keep running on their own after the batch is gone
+        engs[1].run(0)
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_batch_and_solo_steps_interleave():
+    probs = _members(40)
+    ref = []
+    for p in probs[:2]:
+        with Engine(p, "f32-table") as e:
+            e.run(40)
+            ref.append(_state(e))
+    engs = [Engine(p, "f32-table") for p in probs[:2]]
+    try:
+        engs[0].run(10)
+        engs[1].run(10)
+        with Batch(engs) as b:
+            b.run(20)
+        engs[0].run(10)
+        engs[1].run(10)
+        for q in range(2):
+            _assert_same(ref[q], _state(engs[q]), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_batch_argument_errors():
+    probs = _members(30)
+    a = Engine(probs[0], "f32-table")
+    b = Engine(probs[1], "f32-table")
+    c = Engine(probs[2], "f64")
+    try:
+        with pytest.raises(N.FdtdError) as ei:
+            Batch([a, c])
+        assert ei.value.code == N.FDTD_ERR_BADARG
+        with pytest.raises(N.FdtdError) as ei:
+            Batch([a, a])
+        assert ei.value.code == N.FDTD_ERR_BADARG
+        with Batch([a, b]) as bt:
+            with pytest.raises(N.FdtdError):
+                bt.set_tiling(0, 4)
+            with pytest.raises(N.FdtdError):
+                bt.set_tiling(8, 3)
+            a.run(5)
+            with pytest.raises(N.FdtdError) as ei:
+                bt.run(5)
+            assert ei.value.code == N.FDTD_ERR_STATE
+            b.run(5)
+            with pytest.raises(N.FdtdError) as ei:
+                bt.run(26)
+            assert ei.value.code == N.FDTD_ERR_BADARG
+            bt.run(25)
+            assert a.step == b.step == 30
+    finally:
+        for e in (a, b, c):
+            e.close()
+
+
+def test_batch_watchdog_names_the_member():
+    probs = _members(30)[:3]
+    probs[1].voltage_sources[0].voltage_per_e_field[9] = np.nan
+    engs = [Engine(p, "f32-table") for p in probs]
+    try:
+        with Batch(engs) as b:
+            with pytest.raises(N.FdtdError) as ei:
+                b.run(30)
+            assert ei.value.code == N.FDTD_ERR_NONFINITE
+            assert "member 1" in str(ei.value)
+        assert engs[1].status() == (N.FDTD_ERR_NONFINITE, 9)
+        assert engs[0].status() == (0, -1) and engs[2].status() == (0, -1)
+    finally:
+        for e in engs:
+            e.close()
