@@ -253,6 +253,64 @@ int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, doub
 int fdtd_dft_noalloc(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,
                      double* im);
 
+/* ---- learned early stop: a 1-D convolutional network with an MLP head that
+ * reads the first steps of the port transient (no counterpart in the
+ * reference, whose runs always take numberOfTimeSteps steps, index.js:54-60).
+ * Weights enter the arithmetic as BF16 copies of FP32 master values, biases
+ * as FP32; every sum accumulates in FP32.
+ *
+ * Data layout: a sample is `in_length` x `in_channels` values, time major
+ * (channel fastest).  Layers: `conv_layers` convolutions (kernel `kernel`,
+ * stride `stride`, zero padding kernel/2, ReLU) from in_channels to `channels`
+ * channels, the flattened result (time major, channel fastest), `mlp_layers`
+ * dense layers of `mlp_width` with ReLU, and a linear head of `out_dim`.
+ * Flat parameter order: per convolution W[cout][kernel][cin] then b[cout];
+ * per dense layer (the head last) W[out][in] then b[out]. ---- */
+typedef struct fdtd_es_net fdtd_es_net;
+
+typedef struct {
+  int in_channels, in_length;
+  int conv_layers, channels, kernel, stride;
+  int mlp_layers, mlp_width;
+  int out_dim;
+  int max_batch; /* largest batch any call passes */
+  int device;
+} FdtdEsConfig;
+
+int fdtd_es_create(const FdtdEsConfig* cfg, fdtd_es_net** out);
+void fdtd_es_free(fdtd_es_net* net);
+int fdtd_es_param_count(const fdtd_es_net* net, long* count);
+/* Seeded initialisation: every weight and bias uniform in +-1/sqrt(fan_in). */
+int fdtd_es_init_params(fdtd_es_net* net, unsigned long long seed);
+/* FP32 master parameters; setting them also resets the optimiser state. */
+int fdtd_es_set_params(fdtd_es_net* net, const float* params, long count);
+int fdtd_es_get_params(fdtd_es_net* net, float* params, long count);
+/* Forward pass of `batch` samples from host memory; y is batch x out_dim. */
+int fdtd_es_forward(fdtd_es_net* net, const float* x, int batch, float* y);
+/* Loss L = (1/batch) sum_b sum_o w[o] (y[b][o] - target[b][o])^2 and its
+ * gradient with respect to the parameters (grad may be NULL). */
+int fdtd_es_loss_grad(fdtd_es_net* net, const float* x, const float* target, const float* w, int batch,
+                      float* loss, float* grad, long count);
+/* Keeps a training set resident on the device: n samples, targets n x out_dim. */
+int fdtd_es_set_data(fdtd_es_net* net, const float* x, const float* target, long n);
+/* Adam (decoupled weight decay) over the resident set: `epochs` passes of
+ * minibatches of `batch` in a seeded shuffled order (a last partial batch is
+ * dropped); epoch_loss[e] = mean minibatch loss of epoch e (may be NULL). */
+int fdtd_es_train(fdtd_es_net* net, int epochs, int batch, const float* w, float lr, float beta1, float beta2,
+                  float eps, float weight_decay, unsigned long long seed, float* epoch_loss);
+/* Network input built on the device from the port traces of handles (for
+ * handle b: channel 0 = voltage probe 0, channel 1 = current probe 0, over
+ * steps [0, in_length * decim), each value the mean of `decim` consecutive
+ * steps, each channel divided by its largest magnitude; scales[2b] and
+ * scales[2b+1] receive those divisors, 1 for an all-zero channel).  Needs
+ * in_channels == 2 and every handle at step >= in_length * decim.
+ * fdtd_es_member_inputs returns the inputs (x: count x in_length x 2, may be
+ * NULL); fdtd_es_predict_members runs the forward pass on them (y: count x out_dim). */
+int fdtd_es_member_inputs(fdtd_es_net* net, fdtd_ctx* const* members, int count, int decim, float* scales,
+                          float* x);
+int fdtd_es_predict_members(fdtd_es_net* net, fdtd_ctx* const* members, int count, int decim, float* scales,
+                            float* y);
+
 #ifdef __cplusplus
 }
 #endif

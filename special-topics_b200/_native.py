@@ -13,7 +13,9 @@ ROOT = os.path.dirname(PKG_DIR)
 BUILD_DIR = os.path.join(PKG_DIR, "_build")
 LIB_PATH = os.path.join(BUILD_DIR, "libfdtd_b200.so")
 SOURCES = [os.path.join(PKG_DIR, "csrc", f) for f in
-           ("fdtd_b200.cu", "fdtd_common.cuh", "fdtd_step.cuh", "fdtd_material.cuh", "fdtd_batch.cuh")]
+           ("fdtd_b200.cu", "es_net.cu", "fdtd_common.cuh", "fdtd_step.cuh", "fdtd_material.cuh",
+            "fdtd_batch.cuh", "fdtd_internal.h")]
+CU_SOURCES = [p for p in SOURCES if p.endswith(".cu")]
 HEADER = os.path.join(ROOT, "include", "fdtd_b200.h")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -34,6 +36,9 @@ EXPORTS = (
     "fdtd_ctx_read_trace", "fdtd_ctx_read_field", "fdtd_ctx_read_psi", "fdtd_ctx_read_farfield", "fdtd_dft",
     "fdtd_dft_noalloc", "fdtd_batch_create", "fdtd_batch_free", "fdtd_batch_size", "fdtd_batch_set_tiling",
     "fdtd_batch_get_tiling", "fdtd_batch_run", "fdtd_batch_run_timed", "fdtd_batch_profile_kernels",
+    "fdtd_es_create", "fdtd_es_free", "fdtd_es_param_count", "fdtd_es_init_params", "fdtd_es_set_params",
+    "fdtd_es_get_params", "fdtd_es_forward", "fdtd_es_loss_grad", "fdtd_es_set_data", "fdtd_es_train",
+    "fdtd_es_member_inputs", "fdtd_es_predict_members",
 )
 
 
@@ -47,6 +52,11 @@ class FdtdConfig(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
                 ("numberOfTimeSteps", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class FdtdEsConfig(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("in_channels", "in_length", "conv_layers", "channels", "kernel", "stride",
+                                       "mlp_layers", "mlp_width", "out_dim", "max_batch", "device")]
 
 
 class FdtdDims(C.Structure):
@@ -69,7 +79,7 @@ def build(force: bool = False) -> str:
         return LIB_PATH
     os.makedirs(BUILD_DIR, exist_ok=True)
     tmp = LIB_PATH + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", tmp, SOURCES[0]]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", tmp, *CU_SOURCES]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
@@ -127,6 +137,20 @@ def lib() -> C.CDLL:
     L.fdtd_batch_run.argtypes = [v, i]
     L.fdtd_batch_run_timed.argtypes = [v, i, fp]
     L.fdtd_batch_profile_kernels.argtypes = [v, i, dp]
+    L.fdtd_es_create.argtypes = [P(FdtdEsConfig), P(v)]
+    L.fdtd_es_free.argtypes = [v]
+    L.fdtd_es_free.restype = None
+    L.fdtd_es_param_count.argtypes = [v, P(C.c_long)]
+    L.fdtd_es_init_params.argtypes = [v, C.c_ulonglong]
+    L.fdtd_es_set_params.argtypes = [v, fp, lp]
+    L.fdtd_es_get_params.argtypes = [v, fp, lp]
+    L.fdtd_es_forward.argtypes = [v, fp, i, fp]
+    L.fdtd_es_loss_grad.argtypes = [v, fp, fp, fp, i, fp, fp, lp]
+    L.fdtd_es_set_data.argtypes = [v, fp, fp, lp]
+    L.fdtd_es_train.argtypes = [v, i, i, fp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_ulonglong,
+                                fp]
+    L.fdtd_es_member_inputs.argtypes = [v, P(v), i, i, fp, fp]
+    L.fdtd_es_predict_members.argtypes = [v, P(v), i, i, fp, fp]
     L.fdtd_init.argtypes = [P(FdtdDims)]
     L.fdtd_upload_coeff.argtypes = [i, fp, i]
     L.fdtd_upload_cpml.argtypes = [i, i, fp, fp, fp, fp, fp, i, fp, i, fp, i, fp, i, i, i, i]

@@ -17,6 +17,7 @@
 #include "fdtd_material.cuh"
 #include "fdtd_step.cuh"
 #include "fdtd_batch.cuh"
+#include "fdtd_internal.h"
 
 #include <map>
 #include <mutex>
@@ -33,6 +34,8 @@ static int fail(int code, const char* fmt, ...) {
   va_end(ap);
   return code;
 }
+
+int fdtd_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
 #define CK(call)                                                                              \
   do {                                                                                        \
@@ -330,6 +333,20 @@ int check_ready(fdtd_ctx* c) {
   return FDTD_OK;
 }
 
+// True when, on every axis, the two faces' H bands are disjoint and so are
+// their E bands: a position then lies in at most one band per axis.
+int bands_disjoint(const fdtd_ctx* c) {
+  for (int a = 0; a < 3; a++) {
+    const HostFace& n = c->face[2 * a];
+    const HostFace& q = c->face[2 * a + 1];
+    if (!n.present || !q.present || n.nc == 0 || q.nc == 0) continue;
+    const bool h = n.m_start + n.nc <= q.m_start || q.m_start + q.nc <= n.m_start;
+    const bool e = n.e_start + n.nc <= q.e_start || q.e_start + q.nc <= n.e_start;
+    if (!h || !e) return 0;
+  }
+  return 1;
+}
+
 // Kernel parameters shared by both coefficient layouts.
 template <typename T, class C>
 StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
@@ -345,6 +362,7 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   p.dcell[1] = (T)c->dy;
   p.dcell[2] = (T)c->dz;
   p.ichunk = c->ichunk;
+  p.bands_disjoint = bands_disjoint(c);
   return p;
 }
 
@@ -529,6 +547,18 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
 }
 
 }  // namespace
+
+int fdtd_internal_traces(const fdtd_ctx* c, const double** V, const double** I, int* nsteps, int* steps,
+                         int* device) {
+  if (c->vprobe.empty() || c->iprobe.empty())
+    return fail(FDTD_ERR_STATE, "handle has no voltage probe or no current probe");
+  *V = c->V;
+  *I = c->I;
+  *nsteps = c->nsteps;
+  *steps = c->ts;
+  *device = c->device;
+  return FDTD_OK;
+}
 
 // ===========================================================================
 // Handle API

@@ -93,6 +93,16 @@ struct ArrayCoef {
     c1 = r.b;
     c2 = r.c;
   }
+  // get() split into the load (fetch) and this: kappa is in the arrays already
+  __device__ __forceinline__ void decode_k(int comp, const Raw& r, float, float, T& c0, T& c1, T& c2, T& u1,
+                                           T& u2) const {
+    decode(comp, r, c0, c1, c2);
+    u1 = c1;
+    u2 = c2;
+  }
+  // cpsi() split into a load that can be issued early and its use
+  __device__ __forceinline__ T cpsi_fetch(const Face<T>& F, int slot, int pi) const { return F.cpsi[slot][pi]; }
+  __device__ __forceinline__ T cpsi_use(T fetched, T, T) const { return fetched; }
 };
 
 constexpr int kTableRows = 256;
@@ -124,6 +134,15 @@ struct TableCoef {
     c1 = r.y;
     c2 = r.z;
   }
+  // get() split into the id load (fetch) and this row lookup with kappa
+  __device__ __forceinline__ void decode_k(int comp, Raw id, float k1, float k2, float& c0, float& c1, float& c2,
+                                           float& u1, float& u2) const {
+    decode(comp, id, c0, u1, u2);
+    c1 = u1 * k1;
+    c2 = u2 * k2;
+  }
+  __device__ __forceinline__ float cpsi_fetch(const Face<float>&, int, int) const { return 0.f; }
+  __device__ __forceinline__ float cpsi_use(float, float u, float dcell) const { return u * dcell; }
 };
 
 template <typename T, class C>
@@ -137,6 +156,7 @@ struct StepParams {
   Sources<T> src;
   T dcell[3];
   int ichunk;  // x planes per thread
+  int bands_disjoint;  // per axis, no position lies in both CPML bands (H and E)
 };
 
 // Band of a face that contains `pos` (H: m band, E: e band): ci or -1.
@@ -157,6 +177,34 @@ __device__ __forceinline__ void cpml_apply(const C& coef, const Face<T>& F, int 
   P[pi] = ps;
   v = Ar<T, EXACT>::axpy(v, coef.cpsi(F, slot, pi, u, dcell), ps);
 }
+
+// The same correction as cpml_apply with Psi (and CPsi, per-cell layouts)
+// loaded earlier: b and a come from the face's 1-D profiles (cache resident).
+template <typename T, class C, bool EXACT, bool ELECTRIC>
+__device__ __forceinline__ void cpml_apply_loaded(const C& coef, const Face<T>& F, int ci, int pi, int slot, T psi,
+                                                  T cp, T drive, T u, T dcell, T& v) {
+  const T b = ELECTRIC ? F.b_e[ci] : F.b_m[ci];
+  const T a = ELECTRIC ? F.a_e[ci] : F.a_m[ci];
+  const T ps = Ar<T, EXACT>::lin2(b, psi, a, drive);
+  F.psi[slot][pi] = ps;
+  v = Ar<T, EXACT>::axpy(v, coef.cpsi_use(cp, u, dcell), ps);
+}
+
+// Face of axis `a` (0..2) whose band holds `pos`, and the band cell; -1 if none.
+// Only meaningful when the two bands of the axis are disjoint.
+template <typename T>
+__device__ __forceinline__ int band_face(const Face<T>* face, int a, int pos, bool electric, int& ci) {
+  ci = band_ci(face[2 * a], pos, electric);
+  if (ci >= 0) return 2 * a;
+  ci = band_ci(face[2 * a + 1], pos, electric);
+  return ci >= 0 ? 2 * a + 1 : -1;
+}
+
+// Column band state shared by the band loads and stores: y and z faces of the
+// column (-1 if none) and the band cells.
+struct ColBands {
+  int yf, yci, zf, zci;
+};
 
 // Source boxes that contain this thread's (j, k) for component `comp` (bit mask).
 template <typename T>
@@ -327,6 +375,184 @@ __device__ __forceinline__ void h_store(const StepParams<T, C>& p, const HCol<T>
   ey_c = in.ey_n;
 }
 
+// Every input of one H plane of a column in the full form (CPML bands, kappa),
+// so that all loads of a plane can be issued before any of its stores.
+template <typename T, class C>
+struct HBand {
+  HIn<T, C> v;          // field values and coefficient raws
+  float kmx;            // 1/kappa_m at plane i
+  int xf, xci;          // x band of plane i: face and cell, or -1
+  T pa[3], pb[3];       // Psi of the first / second correcting face of Hx, Hy, Hz
+  T ca[3], cb[3];       // their CPsi (per-cell layouts; unused with tables)
+};
+
+template <typename T, class C>
+__device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
+                                            HBand<T, C>& in) {
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  in.xf = band_face(p.face, 0, i, false, in.xci);
+  in.kmx = p.coef.invk(3, i);
+  in.v.ez_n = T(0);
+  in.v.ey_n = T(0);
+  if (c.hx_ok) {
+    const int idx = i * sHx + c.oa;
+    in.v.hx = f.Hx[idx];
+    in.v.ey_kp = f.Ey[i * sHzEy + c.ob + 1];
+    in.v.ez_jp = f.Ez[i * sHyEz + c.oa + nz];
+    in.v.r0 = p.coef.fetch(0, idx);
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      const int pi = (i * F.nc + cb.yci) * nz + c.k;
+      in.pa[0] = F.psi[0][pi];
+      in.ca[0] = p.coef.cpsi_fetch(F, 0, pi);
+    }
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      const int pi = (i * ny + c.j) * F.nc + cb.zci;
+      in.pb[0] = F.psi[0][pi];
+      in.cb[0] = p.coef.cpsi_fetch(F, 0, pi);
+    }
+  }
+  if (i < nx) {
+    const int ex = i * sEx + c.ob;
+    in.v.ex = f.Ex[ex];
+    if (c.hy_ok) {
+      const int idx = i * sHyEz + c.oa;
+      in.v.hy = f.Hy[idx];
+      in.v.ex_kp = f.Ex[ex + 1];
+      in.v.ez_n = f.Ez[idx + sHyEz];
+      in.v.r1 = p.coef.fetch(1, idx);
+      if (in.xf >= 0) {
+        const Face<T>& F = p.face[in.xf];
+        const int pi = in.xci * sHyEz + c.oa;
+        in.pa[1] = F.psi[0][pi];
+        in.ca[1] = p.coef.cpsi_fetch(F, 0, pi);
+      }
+      if (cb.zf >= 0) {
+        const Face<T>& F = p.face[cb.zf];
+        const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
+        in.pb[1] = F.psi[1][pi];
+        in.cb[1] = p.coef.cpsi_fetch(F, 1, pi);
+      }
+    }
+    if (c.hz_ok) {
+      const int idx = i * sHzEy + c.ob;
+      in.v.hz = f.Hz[idx];
+      in.v.ex_jp = f.Ex[ex + nzp1];
+      in.v.ey_n = f.Ey[idx + sHzEy];
+      in.v.r2 = p.coef.fetch(2, idx);
+      if (in.xf >= 0) {
+        const Face<T>& F = p.face[in.xf];
+        const int pi = in.xci * sHzEy + c.ob;
+        in.pa[2] = F.psi[1][pi];
+        in.ca[2] = p.coef.cpsi_fetch(F, 1, pi);
+      }
+      if (cb.yf >= 0) {
+        const Face<T>& F = p.face[cb.yf];
+        const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
+        in.pb[2] = F.psi[1][pi];
+        in.cb[2] = p.coef.cpsi_fetch(F, 1, pi);
+      }
+    }
+  }
+}
+
+// h_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
+// arithmetic in the identical order.
+template <typename T, class C, bool EXACT>
+__device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
+                                             const HBand<T, C>& in, T& ez_c, T& ey_c) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1;
+  const Fields<T>& f = p.f;
+  const T dx = p.dcell[0], dy = p.dcell[1], dz = p.dcell[2];
+  T c0, c1, c2, u1, u2;
+  if (c.hx_ok) {
+    const T dey = A::dif(in.v.ey_kp, ey_c);
+    const T dez = A::dif(in.v.ez_jp, ez_c);
+    p.coef.decode_k(0, in.v.r0, c.kmz, c.kmy, c0, c1, c2, u1, u2);
+    T h = A::lin3(c0, in.v.hx, c1, dey, c2, dez);
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 0, in.pa[0], in.ca[0],
+                                            dez, u2, dy, h);
+    }
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 0, in.pb[0], in.cb[0],
+                                            dey, u1, dz, h);
+    }
+    f.Hx[i * sHx + c.oa] = h;
+  }
+  if (i < nx) {
+    if (c.hy_ok) {
+      const T dez = A::dif(in.v.ez_n, ez_c);
+      const T dex = A::dif(in.v.ex_kp, in.v.ex);
+      p.coef.decode_k(1, in.v.r1, in.kmx, c.kmz, c0, c1, c2, u1, u2);
+      T h = A::lin3(c0, in.v.hy, c1, dez, c2, dex);
+      if (in.xf >= 0)
+        cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 0, in.pa[1],
+                                              in.ca[1], dez, u1, dx, h);
+      if (cb.zf >= 0) {
+        const Face<T>& F = p.face[cb.zf];
+        cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 1, in.pb[1],
+                                              in.cb[1], dex, u2, dz, h);
+      }
+      f.Hy[i * sHyEz + c.oa] = h;
+    }
+    if (c.hz_ok) {
+      const T dex = A::dif(in.v.ex_jp, in.v.ex);
+      const T dey = A::dif(in.v.ey_n, ey_c);
+      p.coef.decode_k(2, in.v.r2, c.kmy, in.kmx, c0, c1, c2, u1, u2);
+      T h = A::lin3(c0, in.v.hz, c1, dex, c2, dey);
+      if (in.xf >= 0)
+        cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 1, in.pa[2],
+                                              in.ca[2], dey, u2, dx, h);
+      if (cb.yf >= 0) {
+        const Face<T>& F = p.face[cb.yf];
+        cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 1, in.pb[2],
+                                              in.cb[2], dex, u1, dy, h);
+      }
+      f.Hz[i * sHzEy + c.ob] = h;
+    }
+  }
+  ez_c = in.v.ez_n;
+  ey_c = in.v.ey_n;
+}
+
+// Planes [a, b) of a column in the band form: every load of a plane is
+// issued before its stores; with BPF the next plane's loads are also in flight.
+template <typename T, class C, bool EXACT, bool BPF>
+__device__ __forceinline__ void h_band_range(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int a,
+                                             int b, T& ez_c, T& ey_c) {
+  if (a >= b) return;
+  HBand<T, C> cur, nxt;
+  if (!BPF) {
+    for (int i = a; i < b; i++) {
+      h_band_load(p, c, cb, i, cur);
+      h_band_store<T, C, EXACT>(p, c, cb, i, cur, ez_c, ey_c);
+    }
+    return;
+  }
+  h_band_load(p, c, cb, a, cur);
+  for (int i = a; i < b; i++) {
+    if (i + 1 < b) h_band_load(p, c, cb, i + 1, nxt);
+    h_band_store<T, C, EXACT>(p, c, cb, i, cur, ez_c, ey_c);
+    cur = nxt;
+  }
+}
+
+// The band form is used for material-table problems; the per-cell layouts
+// (FP64 drop-in) keep the plane-at-a-time form, which needs fewer registers.
+template <class C>
+struct BandForm {
+  static constexpr bool kUse = C::kTable;
+  static constexpr bool kPrefetch = false;
+};
+
 // Minimum resident 256-thread blocks per SM the register budget is fitted to:
 // FP64 values need twice the registers; a deeper prefetch holds one more plane.
 template <typename T, int PF>
@@ -374,7 +600,16 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
     xa = min(max(i0, lo), i1);
     xb = max(xa, min(i1, hi));
   }
-  for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+  ColBands cb{};
+  constexpr bool BPF = BandForm<C>::kPrefetch;
+  const bool band_form = BandForm<C>::kUse && p.bands_disjoint != 0;
+  if (band_form) {
+    cb.yf = band_face(p.face, 1, j, false, cb.yci);
+    cb.zf = band_face(p.face, 2, k, false, cb.zci);
+    h_band_range<T, C, EXACT, BPF>(p, c, cb, i0, xa, ez_c, ey_c);
+  } else {
+    for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+  }
   if (xa < xb) {
     // software pipeline: plane i+1's loads are in flight while plane i is computed and stored
     // software pipeline: the loads of the next PF planes are in flight while
@@ -393,7 +628,10 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
       if (PF == 2) nxt = nx2;
     }
   }
-  for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+  if (band_form)
+    h_band_range<T, C, EXACT, BPF>(p, c, cb, xb, i1, ez_c, ey_c);
+  else
+    for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
 }
 
 template <typename T, class C, bool EXACT, int PF>
@@ -586,6 +824,177 @@ __device__ __forceinline__ void e_store(const StepParams<T, C>& p, const ECol<T>
   hy_p = in.hy;
 }
 
+// Every input of one E plane of a column in the full form.
+template <typename T, class C>
+struct EBand {
+  T ex, hz_jm, hy_km;   // Ex(i), Hz(i,j-1), Hy(i,k-1)
+  T hz_i, hy_i, hx_c;   // Hz(i), Hy(i) (the reference's reads at i = nx), Hx(i)
+  T ey, hx_km;          // Ey(i), Hx(i,k-1)
+  T ez, hx_jm;          // Ez(i), Hx(i,j-1)
+  typename C::Raw r0, r1, r2;
+  float kex;            // 1/kappa_e at plane i
+  int xf, xci;          // x band of plane i, or -1
+  T pa[3], pb[3];       // Psi of the first / second correcting face of Ex, Ey, Ez
+  T ca[3], cb[3];
+};
+
+template <typename T, class C>
+__device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
+                                            EBand<T, C>& in) {
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  const bool inx = i < nx;
+  in.hz_i = c.ey_ok ? (inx ? f.Hz[i * sHzEy + c.ob] : p.ex0b[c.ob]) : T(0);
+  in.hy_i = c.ez_ok ? (inx ? f.Hy[i * sHyEz + c.oa] : f.Hz[c.oa]) : T(0);
+  in.xf = band_face(p.face, 0, i, true, in.xci);
+  in.kex = p.coef.invk(0, i);
+  in.hx_c = (c.ey_ok && c.ez_ok) ? f.Hx[i * sHx + c.oa] : T(0);
+  if (inx) {
+    const int idx = i * sEx + c.ob;
+    in.ex = f.Ex[idx];
+    if (c.jy) in.hz_jm = f.Hz[i * sHzEy + c.ob - nzp1];
+    if (c.kz) in.hy_km = f.Hy[i * sHyEz + c.oa - 1];
+    in.r0 = p.coef.fetch(3, idx);
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
+      in.pa[0] = F.psi[3][pi];
+      in.ca[0] = p.coef.cpsi_fetch(F, 3, pi);
+    }
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
+      in.pb[0] = F.psi[2][pi];
+      in.cb[0] = p.coef.cpsi_fetch(F, 2, pi);
+    }
+  }
+  if (c.ey_ok) {
+    const int idx = i * sHzEy + c.ob;
+    in.ey = f.Ey[idx];
+    if (c.kz) in.hx_km = f.Hx[i * sHx + c.oa - 1];
+    in.r1 = p.coef.fetch(4, idx);
+    if (in.xf >= 0) {
+      const Face<T>& F = p.face[in.xf];
+      const int pi = in.xci * sHzEy + c.ob;
+      in.pa[1] = F.psi[2][pi];
+      in.ca[1] = p.coef.cpsi_fetch(F, 2, pi);
+    }
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      const int pi = (i * ny + c.j) * F.nc + cb.zci;
+      in.pb[1] = F.psi[3][pi];
+      in.cb[1] = p.coef.cpsi_fetch(F, 3, pi);
+    }
+  }
+  if (c.ez_ok) {
+    const int idx = i * sHyEz + c.oa;
+    in.ez = f.Ez[idx];
+    if (c.jy) in.hx_jm = f.Hx[i * sHx + c.oa - nz];
+    in.r2 = p.coef.fetch(5, idx);
+    if (in.xf >= 0) {
+      const Face<T>& F = p.face[in.xf];
+      const int pi = in.xci * sHyEz + c.oa;
+      in.pa[2] = F.psi[3][pi];
+      in.ca[2] = p.coef.cpsi_fetch(F, 3, pi);
+    }
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      const int pi = (i * F.nc + cb.yci) * nz + c.k;
+      in.pb[2] = F.psi[2][pi];
+      in.cb[2] = p.coef.cpsi_fetch(F, 2, pi);
+    }
+  }
+}
+
+// e_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
+// arithmetic in the identical order.
+template <typename T, class C, bool EXACT>
+__device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
+                                             int ts, const EBand<T, C>& in, T& hz_p, T& hy_p) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<T>& f = p.f;
+  const T dx = p.dcell[0], dy = p.dcell[1], dz = p.dcell[2];
+  T c0, c1, c2, u1, u2;
+  if (i < nx) {
+    T e = in.ex;
+    const T dhz = c.jy ? A::dif(in.hz_i, in.hz_jm) : T(0);
+    const T dhy = c.kz ? A::dif(in.hy_i, in.hy_km) : T(0);
+    p.coef.decode_k(3, in.r0, c.key, c.kez, c0, c1, c2, u1, u2);
+    if (c.jy && c.kz) e = A::lin3(c0, e, c1, dhz, c2, dhy);
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 3, in.pa[0], in.ca[0],
+                                           dhz, u1, dy, e);
+    }
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 2, in.pb[0], in.cb[0],
+                                           dhy, u2, dz, e);
+    }
+    if (c.sx) inject_masked(p.src, c.sx, i, c.j, c.k, ts, e);
+    f.Ex[i * sEx + c.ob] = e;
+  }
+  if (c.ey_ok) {
+    T e = in.ey;
+    const T dhx = c.kz ? A::dif(in.hx_c, in.hx_km) : T(0);
+    const T dhz = i >= 1 ? A::dif(in.hz_i, hz_p) : T(0);
+    p.coef.decode_k(4, in.r1, c.kez, in.kex, c0, c1, c2, u1, u2);
+    if (i >= 1 && c.kz) e = A::lin3(c0, e, c1, dhx, c2, dhz);
+    if (in.xf >= 0)
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 2, in.pa[1],
+                                           in.ca[1], dhz, u2, dx, e);
+    if (cb.zf >= 0) {
+      const Face<T>& F = p.face[cb.zf];
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 3, in.pb[1], in.cb[1],
+                                           dhx, u1, dz, e);
+    }
+    if (c.sy) inject_masked(p.src, c.sy, i, c.j, c.k, ts, e);
+    f.Ey[i * sHzEy + c.ob] = e;
+  }
+  if (c.ez_ok) {
+    T e = in.ez;
+    const T dhy = i >= 1 ? A::dif(in.hy_i, hy_p) : T(0);
+    const T dhx = c.jy ? A::dif(in.hx_c, in.hx_jm) : T(0);
+    p.coef.decode_k(5, in.r2, in.kex, c.key, c0, c1, c2, u1, u2);
+    if (i >= 1 && c.jy) e = A::lin3(c0, e, c1, dhy, c2, dhx);
+    if (in.xf >= 0)
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 3, in.pa[2],
+                                           in.ca[2], dhy, u1, dx, e);
+    if (cb.yf >= 0) {
+      const Face<T>& F = p.face[cb.yf];
+      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 2, in.pb[2], in.cb[2],
+                                           dhx, u2, dy, e);
+    }
+    if (c.sz) inject_masked(p.src, c.sz, i, c.j, c.k, ts, e);
+    f.Ez[i * sHyEz + c.oa] = e;
+  }
+  hz_p = in.hz_i;
+  hy_p = in.hy_i;
+}
+
+template <typename T, class C, bool EXACT, bool BPF>
+__device__ __forceinline__ void e_band_range(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int a,
+                                             int b, int ts, T& hz_p, T& hy_p) {
+  if (a >= b) return;
+  EBand<T, C> cur, nxt;
+  if (!BPF) {
+    for (int i = a; i < b; i++) {
+      e_band_load(p, c, cb, i, cur);
+      e_band_store<T, C, EXACT>(p, c, cb, i, ts, cur, hz_p, hy_p);
+    }
+    return;
+  }
+  e_band_load(p, c, cb, a, cur);
+  for (int i = a; i < b; i++) {
+    if (i + 1 < b) e_band_load(p, c, cb, i + 1, nxt);
+    e_band_store<T, C, EXACT>(p, c, cb, i, ts, cur, hz_p, hy_p);
+    cur = nxt;
+  }
+}
+
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
   const int k = bx * blockDim.x + threadIdx.x;
@@ -627,7 +1036,16 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
     xa = min(max(i0, max(lo, 1)), i1);
     xb = max(xa, min(i1, min(hi, nx)));
   }
-  for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  ColBands cb{};
+  constexpr bool BPF = BandForm<C>::kPrefetch;
+  const bool band_form = BandForm<C>::kUse && p.bands_disjoint != 0;
+  if (band_form) {
+    cb.yf = band_face(p.face, 1, j, true, cb.yci);
+    cb.zf = band_face(p.face, 2, k, true, cb.zci);
+    e_band_range<T, C, EXACT, BPF>(p, c, cb, i0, xa, ts, hz_p, hy_p);
+  } else {
+    for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  }
   if (xa < xb) {
     EIn<T, C> cur, nxt, nx2;
     e_load(p, c, xa, cur);
@@ -643,7 +1061,10 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
       if (PF == 2) nxt = nx2;
     }
   }
-  for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  if (band_form)
+    e_band_range<T, C, EXACT, BPF>(p, c, cb, xb, i1, ts, hz_p, hy_p);
+  else
+    for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
 }
 
 template <typename T, class C, bool EXACT, int PF>

@@ -1,0 +1,92 @@
+"""CPU checks of the early-stop network's FP64 oracle and of the host-side
+tail model (no GPU): BF16 rounding against torch's, the oracle's analytic
+backward pass against finite differences, and mode fitting on synthetic
+ringing with known parameters."""
+import numpy as np
+import pytest
+import torch
+
+import es_net_oracle as O
+from conftest import load_package
+
+pkg = load_package()
+from special_topics_b200 import earlystop as ES  # noqa: E402
+
+SMALL = dict(in_channels=2, in_length=23, conv_layers=2, channels=4, kernel=5, stride=2, mlp_layers=1,
+             mlp_width=8)
+
+
+def test_bf16_round_matches_torch():
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.standard_normal(20000) * 10.0 ** rng.integers(-30, 30, 20000),
+                        [0.0, -0.0, 1.0, 1.00390625, 1.01171875, 3.4e38, -3.4e38, 1e-40, np.inf, -np.inf]])
+    x = x.astype(np.float32)
+    ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy()
+    assert np.array_equal(O.bf16_round(x).view(np.uint32), ref.view(np.uint32))
+    assert np.isnan(O.bf16_round(np.array([np.nan], np.float32)))[0]
+
+
+def test_layer_table_and_param_count():
+    Ls = O.layers(O.DEFAULT_ARCH, 6)
+    assert [L["lout"] for L in Ls if L["conv"]] == [188, 94, 47, 24]
+    assert O.param_count(O.DEFAULT_ARCH, 6) == (64 * 5 * 2 + 64) + 3 * (64 * 5 * 64 + 64) + (1536 * 256 + 256) \
+        + (256 * 256 + 256) + (256 * 6 + 6)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_oracle_backward_matches_finite_differences(seed):
+    rng = np.random.default_rng(seed)
+    n = O.param_count(SMALL, 3)
+    p = rng.uniform(-0.5, 0.5, n)
+    x = rng.standard_normal((5, SMALL["in_length"], 2))
+    t = rng.standard_normal((5, 3))
+    w = np.array([1.0, 0.5, 2.0])
+    loss, g = O.loss_grad(SMALL, 3, p, x, t, w, bf16=False)
+    assert abs(loss - O.loss(SMALL, 3, p, x, t, w, bf16=False)) < 1e-12
+    idx = rng.choice(n, 60, replace=False)
+    fd = O.finite_difference(SMALL, 3, p, x, t, w, idx)
+    assert np.allclose(g[idx], fd, rtol=1e-5, atol=1e-8), np.abs(g[idx] - fd).max()
+
+
+def test_inputs_from_traces_scales_each_channel():
+    rng = np.random.default_rng(3)
+    V, I = rng.standard_normal(1600), 0.01 * rng.standard_normal(1600)
+    x, s = ES.inputs_from_traces(V, I)
+    assert x.shape == (375, 2) and x.dtype == np.float32
+    assert np.isclose(np.abs(x).max(axis=0), 1.0).all()
+    assert np.isclose(s[0], np.abs(V[:1500].reshape(375, 4).mean(1)).max())
+
+
+def _ringing(m, n, extra=None, dt=8.666e-13):
+    V, I = m.eval("V", np.arange(n), dt), m.eval("I", np.arange(n), dt)
+    if extra is not None:
+        V = V + extra.eval("V", np.arange(n), dt)
+        I = I + extra.eval("I", np.arange(n), dt)
+    return V, I
+
+
+def test_dominant_mode_recovers_a_damped_sinusoid():
+    dt = 8.666e-13
+    m0 = ES.Mode(2.17e9, 0.46e9, 0.011 - 0.004j, 1.5e-4 + 2e-5j, 1500)
+    V, I = _ringing(m0, 7000, extra=ES.Mode(4.9e9, 2.5e9, 0.002, 3e-5, 1500))
+    m = ES.dominant_mode(V, I, 1500, 7000, dt)
+    assert abs(m.f - m0.f) < 1e3 and abs(m.alpha - m0.alpha) < 1e3
+    assert abs(m.cV - m0.cV) < 1e-6 and abs(m.cI - m0.cI) < 1e-8
+    y = ES.mode_to_target(m, (0.02, 3e-4))
+    back = ES.target_to_mode(y, (0.02, 3e-4), 1500)
+    assert abs(back.f - m.f) < 1e3 and abs(back.alpha / m.alpha - 1) < 1e-6
+
+
+def test_refit_residual_separates_one_mode_from_two():
+    dt = 8.666e-13
+    m = ES.Mode(2.17e9, 0.46e9, 0.011, 1.5e-4, 1500)
+    V, I = _ringing(m, 2000)
+    guess = ES.Mode(m.f, m.alpha, 0j, 0j, 1500)
+    got, r = ES.refit(V, I, guess, 2000, dt)
+    assert r < 1e-20 and abs(got.cV - m.cV) < 1e-12
+    V2, I2 = _ringing(m, 2000, extra=ES.Mode(3.1e9, 0.2e9, 0.008, 1e-4, 1500))
+    _, r2 = ES.refit(V2, I2, guess, 2000, dt)
+    assert r2 > 0.05
+    Ve, _ = ES.extend(V, I, got, 1800, 7000, dt)
+    full_V, _ = _ringing(m, 7000)
+    assert len(Ve) == 7000 and np.allclose(Ve, full_V, atol=1e-12)
