@@ -233,6 +233,13 @@ int fdtd_ctx_read_psi(fdtd_ctx* ctx, int faceId, int slot, double* host, long n)
  * cmxzp cmyzp cmxzn cmyzn), laid out [freq][point] like farfield.js:55. */
 int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, long n);
 
+/* Far-field post-processing on the device from the handle's accumulators
+ * (farfield.js:257-607): radp[f] = radiated power at frequency f, and the
+ * directivity components d_theta / d_phi [nFreq][nang] towards the nang
+ * directions (theta[a], phi[a]) in radians (nang may be 0). */
+int fdtd_ctx_farfield_post(fdtd_ctx* ctx, const double* theta, const double* phi, int nang, double* radp,
+                           double* d_theta, double* d_phi);
+
 /* Direct time-to-frequency transform on the device (dft.js:17-38):
  * X(f) = dt * sum_n x[n] exp(-j 2 pi f ((n+1) dt + shift)), FP64. */
 int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,

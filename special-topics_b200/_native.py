@@ -14,7 +14,7 @@ BUILD_DIR = os.path.join(PKG_DIR, "_build")
 LIB_PATH = os.path.join(BUILD_DIR, "libfdtd_b200.so")
 SOURCES = [os.path.join(PKG_DIR, "csrc", f) for f in
            ("fdtd_b200.cu", "es_net.cu", "fdtd_common.cuh", "fdtd_step.cuh", "fdtd_material.cuh",
-            "fdtd_batch.cuh", "fdtd_internal.h")]
+            "fdtd_batch.cuh", "fdtd_internal.h", "fdtd_ffpost.cuh")]
 CU_SOURCES = [p for p in SOURCES if p.endswith(".cu")]
 HEADER = os.path.join(ROOT, "include", "fdtd_b200.h")
 
@@ -38,7 +38,7 @@ EXPORTS = (
     "fdtd_batch_get_tiling", "fdtd_batch_run", "fdtd_batch_run_timed", "fdtd_batch_profile_kernels",
     "fdtd_es_create", "fdtd_es_free", "fdtd_es_param_count", "fdtd_es_init_params", "fdtd_es_set_params",
     "fdtd_es_get_params", "fdtd_es_forward", "fdtd_es_loss_grad", "fdtd_es_set_data", "fdtd_es_train",
-    "fdtd_es_member_inputs", "fdtd_es_predict_members",
+    "fdtd_es_member_inputs", "fdtd_es_predict_members", "fdtd_ctx_farfield_post",
 )
 
 
@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_read_psi.argtypes = [v, i, i, dp, lp]
     L.fdtd_ctx_read_farfield.argtypes = [v, i, dp, dp, lp]
     L.fdtd_dft.argtypes = [dp, i, d, dp, i, d, dp, dp]
+    L.fdtd_ctx_farfield_post.argtypes = [v, dp, dp, i, dp, dp, dp]
     L.fdtd_dft_noalloc.argtypes = [dp, i, d, dp, i, d, dp, dp]
     L.fdtd_batch_create.argtypes = [P(v), i, P(v)]
     L.fdtd_batch_free.argtypes = [v]

@@ -184,6 +184,21 @@ class Engine:
             out[name] = (re, im)
         return out
 
+    def farfield_post(self, theta, phi):
+        """Radiated power [nFreq] and directivity D_theta, D_phi [nFreq, nang]
+        computed on the device from the accumulators (farfield.js:257-607)."""
+        theta = np.ascontiguousarray(theta, dtype=np.float64).ravel()
+        phi = np.ascontiguousarray(phi, dtype=np.float64).ravel()
+        if theta.shape != phi.shape:
+            raise ValueError("theta and phi must have the same length")
+        nf = self.problem.farfield.nFreq if self.problem.farfield is not None else 0
+        radp = np.zeros(max(nf, 1))
+        dth = np.zeros((max(nf, 1), theta.size))
+        dph = np.zeros((max(nf, 1), theta.size))
+        N.check(N.lib().fdtd_ctx_farfield_post(self._h, N.dptr(theta), N.dptr(phi), theta.size, N.dptr(radp),
+                                               N.dptr(dth), N.dptr(dph)))
+        return radp[:nf], dth[:nf], dph[:nf]
+
     def close(self) -> None:
         h = getattr(self, "_h", None)
         if h is not None and h.value:

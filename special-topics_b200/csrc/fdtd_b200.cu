@@ -17,6 +17,7 @@
 #include "fdtd_material.cuh"
 #include "fdtd_step.cuh"
 #include "fdtd_batch.cuh"
+#include "fdtd_ffpost.cuh"
 #include "fdtd_internal.h"
 
 #include <map>
@@ -110,6 +111,7 @@ struct fdtd_ctx {
   int li = 0, lj = 0, lk = 0, ui = 0, uj = 0, uk = 0;
   double* ph = nullptr;
   double* acc = nullptr;
+  std::vector<double> ffreq;  // far-field frequencies (Hz)
   long long ffsz[3] = {};
   long long ffoff[24] = {};
   void* ex0b = nullptr;
@@ -824,6 +826,7 @@ int fdtd_ctx_setup_farfield(fdtd_ctx* c, int nFreq, const double* freqs, int li,
     return fail(FDTD_ERR_BADARG, "Huygens box [%d,%d]x[%d,%d]x[%d,%d] does not fit the grid", li, ui, lj, uj, lk, uk);
   CK(cudaSetDevice(c->device));
   c->nFreq = nFreq;
+  c->ffreq.assign(freqs, freqs + nFreq);
   c->li = li; c->lj = lj; c->lk = lk; c->ui = ui; c->uj = uj; c->uk = uk;
   const long long ni = ui - li, nj = uj - lj, nk = uk - lk;
   c->ffsz[0] = nj * nk;
@@ -1193,6 +1196,72 @@ int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, doub
   cudaFree(dx_);
   cudaFree(df);
   cudaFree(dr);
+  return rc;
+}
+
+int fdtd_ctx_farfield_post(fdtd_ctx* c, const double* theta, const double* phi, int nang, double* radp,
+                           double* d_theta, double* d_phi) {
+  if (!c || !radp || (nang > 0 && (!theta || !phi || !d_theta || !d_phi)) || nang < 0)
+    return fail(FDTD_ERR_BADARG, "bad far-field post arguments");
+  if (c->nFreq == 0) return fail(FDTD_ERR_STATE, "no far field set up");
+  CK(cudaSetDevice(c->device));
+  FFPost P{};
+  P.acc = c->acc;
+  for (int a = 0; a < 24; a++) P.off[a] = c->ffoff[a];
+  for (int a = 0; a < 3; a++) P.sz[a] = c->ffsz[a];
+  P.nFreq = c->nFreq;
+  P.ni = c->ui - c->li;
+  P.nj = c->uj - c->lj;
+  P.nk = c->uk - c->lk;
+  const double d[3] = {c->dx, c->dy, c->dz};
+  const int lo[3] = {c->li, c->lj, c->lk}, hi[3] = {c->ui, c->uj, c->uk};
+  for (int a = 0; a < 3; a++) {
+    const double centre = 0.5 * (hi[a] + lo[a]);
+    P.d[a] = d[a];
+    P.pos0[a] = ((lo[a] - 1) - centre + 0.5) * d[a];
+    P.face[a][0] = (hi[a] - centre) * d[a];
+    P.face[a][1] = (lo[a] - centre) * d[a];
+  }
+  const int F = c->nFreq;
+  double *dfreq = nullptr, *dradp = nullptr, *dang = nullptr, *dout = nullptr;
+  int rc = FDTD_OK;
+  const size_t na = (size_t)std::max(nang, 1);
+  if (cudaMalloc(&dfreq, F * sizeof(double)) != cudaSuccess || cudaMalloc(&dradp, F * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&dang, 2 * na * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&dout, 2 * F * na * sizeof(double)) != cudaSuccess) {
+    rc = fail(FDTD_ERR_OOM, "far-field post buffers");
+  }
+  cudaError_t e = cudaSuccess;
+  if (!rc) {
+    e = cudaMemcpyAsync(dfreq, c->ffreq.data(), F * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nang > 0)
+      e = cudaMemcpyAsync(dang, theta, nang * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nang > 0)
+      e = cudaMemcpyAsync(dang + na, phi, nang * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+      k_ff_power<<<F, 256, 0, c->stream>>>(P, dradp);
+      if (nang > 0) {
+        const dim3 grd((nang + 256 * kFFAng - 1) / (256 * kFFAng), F);
+        k_ff_pattern<<<grd, 256, 0, c->stream>>>(P, dfreq, dang, dang + na, nang, dradp, dout, dout + F * na);
+      }
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(radp, dradp, F * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && nang > 0)
+      for (int f = 0; f < F && e == cudaSuccess; f++) {
+        e = cudaMemcpyAsync(d_theta + (size_t)f * nang, dout + f * na, nang * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_phi + (size_t)f * nang, dout + F * na + f * na, nang * sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream);
+      }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "far-field post: %s", cudaGetErrorString(e));
+  }
+  cudaFree(dfreq);
+  cudaFree(dradp);
+  cudaFree(dang);
+  cudaFree(dout);
   return rc;
 }
 

@@ -52,6 +52,22 @@ class EsNet:
         n = C.c_long()
         N.check(N.lib().fdtd_es_param_count(self._h, C.byref(n)))
         self.n_params = n.value
+        # targets are learned standardised: raw = out * out_sd + out_mu (FP32, outside the network)
+        self.out_mu = np.zeros(out_dim, np.float32)
+        self.out_sd = np.ones(out_dim, np.float32)
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.params, out_mu=self.out_mu, out_sd=self.out_sd, out_dim=self.out_dim,
+                 **{k: v for k, v in self.arch.items()})
+
+    @classmethod
+    def load(cls, path: str, max_batch: int = 512, device: int = 0) -> "EsNet":
+        z = np.load(path)
+        arch = {k: int(z[k]) for k in ARCH}
+        net = cls(int(z["out_dim"]), max_batch=max_batch, device=device, **arch)
+        net.params = z["params"]
+        net.out_mu, net.out_sd = z["out_mu"].astype(np.float32), z["out_sd"].astype(np.float32)
+        return net
 
     def init(self, seed: int = 0) -> None:
         N.check(N.lib().fdtd_es_init_params(self._h, int(seed)))
@@ -111,11 +127,13 @@ class EsNet:
         return x, scales.reshape(-1, 2)
 
     def predict_members(self, engines, decim: int = DECIM):
+        """Raw targets (standardisation undone) predicted from the engines'
+        device traces, and the input scales of each engine."""
         arr = self._members(engines)
         scales = np.zeros(2 * len(engines), np.float32)
         y = np.zeros((len(engines), self.out_dim), np.float32)
         N.check(N.lib().fdtd_es_predict_members(self._h, arr, len(engines), decim, N.fptr(scales), N.fptr(y)))
-        return y, scales.reshape(-1, 2)
+        return y * self.out_sd + self.out_mu, scales.reshape(-1, 2)
 
     def close(self) -> None:
         h = getattr(self, "_h", None)
@@ -298,3 +316,93 @@ def run_variants(problems, steps: int, precision: str = "f32-table", group: int 
             for e in engs:
                 e.close()
     return V, I, device_s
+
+
+# ---------------------------------------------------------------------------
+# Stopping runs early
+# ---------------------------------------------------------------------------
+@dataclass
+class StopPolicy:
+    """n_in: steps the network reads; n_check: steps run past n_in whose
+    samples refit the amplitudes and measure the residual; max_resid: the
+    residual-energy ratio above which a run is not stopped; n_total: the
+    step count the result stands in for (numberOfTimeSteps)."""
+    n_in: int = 1500
+    n_check: int = 300
+    max_resid: float = 0.03
+    n_total: int = 7000
+    decim: int = DECIM
+
+    @property
+    def n_stop(self) -> int:
+        return self.n_in + self.n_check
+
+
+def pencil_mode(V, I, n0: int, n1: int, dt: float, decim: int = DECIM) -> Mode:
+    """The method without the network: the dominant mode estimated from the
+    run's own samples [n0, n1) by the joint matrix pencil."""
+    return dominant_mode(V, I, n0, n1, dt, decim=decim)
+
+
+def decide(V, I, mode: Mode | None, policy: StopPolicy, dt: float):
+    """Refits `mode` on [n_in, n_stop) and applies the residual-energy gate.
+    Returns (accepted, refitted mode or None, residual)."""
+    if mode is None or not (mode.alpha > 0 and math.isfinite(mode.f)):
+        return False, None, float("inf")
+    m, r = refit(V, I, mode, policy.n_stop, dt)
+    return r <= policy.max_resid, m, r
+
+
+def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: dict | None = None,
+                        use_network: bool = True) -> list[dict]:
+    """Advances FP32 engines of one batch to policy.n_stop, predicts each run's
+    tail mode (the network, or the pencil on the run's own samples when
+    use_network is False), and stops the runs whose refit passes the gate;
+    the others keep stepping to n_total (plain FDTD).  Returns per engine
+    {"V", "I": traces over n_total steps (stopped runs extended with their
+    tail), "stopped_at", "accepted", "resid", "mode"}."""
+    from .backend import Batch
+    with Batch(engines) as b:
+        if tiling:
+            b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+        b.run(policy.n_stop - b.step)
+    modes = [None] * len(engines)
+    if use_network:
+        y, scales = net.predict_members(engines, policy.decim)
+        modes = [target_to_mode(y[q], scales[q], policy.n_in) for q in range(len(engines))]
+    out, rest = [], []
+    for q, e in enumerate(engines):
+        dt = e.problem.grid.dt
+        V, I = e.voltages(policy.n_stop)[0], e.currents(policy.n_stop)[0]
+        m = modes[q]
+        if not use_network:
+            try:
+                m = pencil_mode(V, I, policy.n_in, policy.n_stop, dt, policy.decim)
+            except (ValueError, np.linalg.LinAlgError):
+                m = None
+        ok, fit, r = decide(V, I, m, policy, dt)
+        rec = {"accepted": ok, "resid": r, "mode": fit, "stopped_at": policy.n_stop}
+        if ok:
+            rec["V"], rec["I"] = extend(V, I, fit, policy.n_stop, policy.n_total, dt)
+        else:
+            rest.append(q)
+        out.append(rec)
+    if rest:
+        with Batch([engines[q] for q in rest]) as b:
+            if tiling:
+                b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+            b.run(policy.n_total - b.step)
+        for q in rest:
+            e = engines[q]
+            out[q]["V"], out[q]["I"] = e.voltages(policy.n_total)[0], e.currents(policy.n_total)[0]
+            out[q]["stopped_at"] = policy.n_total
+    return out
+
+
+def s11_db(V, I, dt: float, freqs, z0: float = 50.0) -> np.ndarray:
+    """|S11| in dB of one port from its traces (postproc.port_s11, GPU DFT)."""
+    from . import postproc
+    return postproc.port_s11(V, I, dt, freqs, z0)["mag_dB"]
+
+
+S11_FREQS = np.linspace(1e9, 4e9, 301)

@@ -1,0 +1,173 @@
+"""Trains and evaluates the learned early stop on the inverted-F variant family.
+
+  python special-topics_b200/train_earlystop.py --out DIR [--train 4096] [--test 512] [--epochs 200]
+
+1. Transients: the batched FP32 solver runs every training variant
+   (seeds 1000..) for the full step count; the port V/I traces are kept.
+2. Labels: the dominant tail mode of each run, fitted on [n_in, n_total) of
+   its own traces (earlystop.dominant_mode); inputs: the first n_in steps,
+   4x decimated and scaled (earlystop.inputs_from_traces, the same values the
+   device input builder produces).
+3. Training: the CUDA network (fdtd_es_train, Adam, BF16 weights) on those
+   pairs, in stages of decreasing learning rate.
+4. Evaluation on held-out seeds (10000..): plain FP64 batched runs of the full
+   step count give the reference S11 (301 points, 1-4 GHz) and the plain
+   time-to-S11; the FP32 runs stopped early by the network, and the same
+   stopping rule with the network replaced by a pencil fit on the run's own
+   samples, give theirs.  Reported: the share of runs within 0.1 dB (max over
+   the 301 points), time-to-S11 of each method, steps run.
+
+Writes DIR/es_weights.npz (EsNet.save: parameters, architecture, target
+scaling) and DIR/es_metrics.json.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import multiprocessing as mp
+import os
+import sys
+import time
+
+import numpy as np
+
+
+def _package():
+    name = "special_topics_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    d = os.path.dirname(os.path.abspath(__file__))
+    spec = importlib.util.spec_from_file_location(name, os.path.join(d, "__init__.py"), submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules[name] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def _label(args):
+    V, I, n0, n1, dt = args
+    _package()
+    from special_topics_b200 import earlystop as ES
+    try:
+        return ES.dominant_mode(V, I, n0, n1, dt)
+    except (ValueError, np.linalg.LinAlgError):
+        return None
+
+
+def build_set(ES, pool, seeds, steps, policy, tiling):
+    probs = ES.variant_problems(seeds, steps, pool)
+    V, I, dev_s = ES.run_variants(probs, steps, "f32-table", tiling=tiling)
+    dts = [p.grid.dt for p in probs]
+    modes = pool.map(_label, [(V[q], I[q], policy.n_in, steps, dts[q]) for q in range(len(seeds))])
+    x, y, keep = [], [], []
+    for q, m in enumerate(modes):
+        if m is None:
+            continue
+        xi, sc = ES.inputs_from_traces(V[q], I[q], ES.ARCH["in_length"], policy.decim)
+        x.append(xi)
+        y.append(ES.mode_to_target(m, sc))
+        keep.append(q)
+    return np.array(x, np.float32), np.array(y, np.float32), keep, dev_s
+
+
+def evaluate(ES, pool, seeds, net, policy, tiling, group=128):
+    """Plain FP64 reference vs the early-stopped FP32 runs (with and without the network)."""
+    from special_topics_b200.backend import Batch, Engine
+    probs = ES.variant_problems(seeds, policy.n_total, pool)
+    freqs = ES.S11_FREQS
+    ref, t_plain = [], 0.0
+    for g0 in range(0, len(probs), group):
+        engs = [Engine(p, "f64") for p in probs[g0:g0 + group]]
+        try:
+            t0 = time.perf_counter()
+            with Batch(engs) as b:
+                if tiling:
+                    b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+                b.run(policy.n_total)
+            for e in engs:
+                ref.append(ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs))
+            t_plain += time.perf_counter() - t0
+        finally:
+            for e in engs:
+                e.close()
+    out = {"plain_f64": {"time_s": t_plain, "steps": policy.n_total * len(probs)}}
+    for name, use_net in (("learned", True), ("no_network", False)):
+        errs, stops, t = [], [], 0.0
+        for g0 in range(0, len(probs), group):
+            engs = [Engine(p, "f32-table") for p in probs[g0:g0 + group]]
+            try:
+                t0 = time.perf_counter()
+                res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use_net)
+                s11 = [ES.s11_db(r["V"], r["I"], e.problem.grid.dt, freqs) for r, e in zip(res, engs)]
+                t += time.perf_counter() - t0
+            finally:
+                for e in engs:
+                    e.close()
+            for q, r in enumerate(res):
+                errs.append(float(np.abs(s11[q] - ref[g0 + q]).max()))
+                stops.append(r["stopped_at"])
+        errs = np.array(errs)
+        out[name] = {"time_s": t, "steps": int(np.sum(stops)), "stopped_early": int(np.sum(np.array(stops) < policy.n_total)),
+                     "within_0p1_dB": float(np.mean(errs <= 0.1)), "max_err_dB_median": float(np.median(errs)),
+                     "max_err_dB_p90": float(np.percentile(errs, 90)), "max_err_dB_worst": float(errs.max())}
+    out["time_to_s11_ratio_plain_over_learned"] = out["plain_f64"]["time_s"] / out["learned"]["time_s"]
+    out["time_to_s11_ratio_plain_over_no_network"] = out["plain_f64"]["time_s"] / out["no_network"]["time_s"]
+    out["runs"] = len(probs)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--train", type=int, default=4096)
+    ap.add_argument("--test", type=int, default=512)
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--n-check", type=int, default=300)
+    ap.add_argument("--max-resid", type=float, default=0.03)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
+    _package()
+    from special_topics_b200 import earlystop as ES
+    policy = ES.StopPolicy(n_check=args.n_check, max_resid=args.max_resid)
+    tiling = dict(chunk=16, rows=4, prefetch=1, group=0)
+    metrics = {"policy": policy.__dict__, "arch": ES.ARCH}
+    t0 = time.perf_counter()
+    x, y, keep, dev_s = build_set(ES, pool, range(1000, 1000 + args.train), policy.n_total, policy, tiling)
+    metrics["train_set"] = {"runs": args.train, "labelled": len(keep), "solver_device_s": dev_s,
+                            "wall_s": time.perf_counter() - t0}
+    # target scaling: each output standardised over the training set
+    mu, sd = y.mean(axis=0), y.std(axis=0) + 1e-6
+    yn = (y - mu) / sd
+    n_val = max(1, len(x) // 16)
+    xv, yv = x[:n_val], yn[:n_val]
+    net = ES.EsNet(max_batch=512)
+    net.init(args.seed)
+    losses = []
+    t0 = time.perf_counter()
+    w = np.array([4.0, 2.0, 1.0, 1.0, 1.0, 1.0], np.float32)   # the pole matters most
+    for stage, lr in enumerate((1e-3, 3e-4, 1e-4)):
+        ep = args.epochs // 3
+        losses += net.train(x[n_val:], yn[n_val:], epochs=ep, batch=args.batch, w=w, lr=lr, weight_decay=1e-4,
+                            seed=args.seed + stage).tolist()
+    metrics["training"] = {"wall_s": time.perf_counter() - t0, "epochs": len(losses), "first_loss": losses[0],
+                           "last_loss": losses[-1], "val_loss": net.loss_grad(xv, yv, w, grad=False)[0]}
+    pv = net.forward(xv) * sd + mu
+    metrics["val_pole_err"] = {"f_rel_median": float(np.median(np.abs(pv[:, 0] - y[:n_val, 0]) * ES.F_SCALE
+                                                               / (y[:n_val, 0] * ES.F_SCALE + ES.F_CENTER))),
+                               "alpha_rel_median": float(np.median(np.abs(np.exp(pv[:, 1] - y[:n_val, 1]) - 1)))}
+    net.out_mu, net.out_sd = mu.astype(np.float32), sd.astype(np.float32)
+    net.save(os.path.join(args.out, "es_weights.npz"))
+    metrics["evaluation"] = evaluate(ES, pool, range(10000, 10000 + args.test), net, policy, tiling)
+    with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
+        json.dump(metrics, f, indent=1)
+    print(json.dumps(metrics["evaluation"]), flush=True)
+    pool.close()
+    net.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -240,3 +240,23 @@ def test_autotuner_picks_a_measured_shape(tmp_path, monkeypatch):
     res = autotune.tune(p, "f32-table", steps_per_candidate=8)
     assert {"chunk", "rows", "ms_per_step"} <= set(res)
     assert res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
+
+
+@pytest.mark.parametrize("name", ["ifa-fr4-substrate", "small-yn"])
+def test_device_farfield_post_matches_host(name):
+    """Radiated power and directivity on the device against postproc's FP64
+    host restatement of farfield.js:257-607, on the same accumulators."""
+    scn, steps = CASES[name]()
+    p = build_problem_from_scenario(scn, steps)
+    with Engine(p, "f64") as eng:
+        eng.run(steps)
+        acc = eng.farfield()
+        radp_h = postproc.radiated_power(acc, p.grid, p.farfield)
+        th = np.radians(np.arange(0, 181, 7.0))
+        ph = np.radians(np.arange(0, 360, 11.0))
+        T, P = [a.ravel() for a in np.meshgrid(th, ph, indexing="ij")]
+        dth_h, dph_h = postproc.directivity(acc, p.grid, p.farfield, radp_h, T, P)
+        radp, dth, dph = eng.farfield_post(T, P)
+        assert np.allclose(radp, radp_h, rtol=1e-10, atol=0)
+        for d, h in ((dth, dth_h), (dph, dph_h)):
+            assert np.abs(d - h).max() <= 1e-9 * np.abs(h).max()
