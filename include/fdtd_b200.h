@@ -233,6 +233,12 @@ int fdtd_ctx_read_psi(fdtd_ctx* ctx, int faceId, int slot, double* host, long n)
  * cmxzp cmyzp cmxzn cmyzn), laid out [freq][point] like farfield.js:55. */
 int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, long n);
 
+/* Far-field accumulator arithmetic of an FP32 problem: 0 = FP64 (default),
+ * 1 = Kahan-compensated FP32 pairs (same 8 bytes per value).  Readback
+ * returns FP64 either way.  Set before the first step; FP64 problems keep
+ * FP64.  No counterpart in the reference (its accumulators are Float64Array). */
+int fdtd_ctx_set_dft_accumulator(fdtd_ctx* ctx, int kahan_fp32);
+
 /* Far-field post-processing on the device from the handle's accumulators
  * (farfield.js:257-607): radp[f] = radiated power at frequency f, and the
  * directivity components d_theta / d_phi [nFreq][nang] towards the nang

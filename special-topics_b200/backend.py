@@ -29,10 +29,14 @@ FIELD_IDS = {"Hx": 0, "Hy": 1, "Hz": 2, "Ex": 3, "Ey": 4, "Ez": 5}
 class Engine:
     """One problem resident on one GPU."""
 
-    def __init__(self, problem: Problem, precision: str = "f64", device: int = 0, host_tables: bool = False):
+    def __init__(self, problem: Problem, precision: str = "f64", device: int = 0, host_tables: bool = False,
+                 dft_accumulator: str = "f64"):
         """host_tables=True builds an FP32-table problem's ids with numpy
         (tables.build_tables, needs per-cell material arrays) instead of on the
-        device (fdtd_ctx_build_material)."""
+        device (fdtd_ctx_build_material).  dft_accumulator "kahan-f32" keeps an
+        FP32 problem's far-field accumulators as compensated FP32 pairs."""
+        if dft_accumulator not in ("f64", "kahan-f32"):
+            raise ValueError("dft_accumulator must be 'f64' or 'kahan-f32'")
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         L = N.lib()
@@ -47,6 +51,8 @@ class Engine:
         self._h = h
         try:
             self._upload()
+            if dft_accumulator == "kahan-f32":
+                N.check(L.fdtd_ctx_set_dft_accumulator(h, 1))
         except Exception:
             self.close()
             raise

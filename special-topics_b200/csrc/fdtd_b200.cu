@@ -112,6 +112,7 @@ struct fdtd_ctx {
   double* ph = nullptr;
   double* acc = nullptr;
   std::vector<double> ffreq;  // far-field frequencies (Hz)
+  int acc_kahan = 0;          // FP32 problems: compensated FP32 accumulator pairs instead of FP64
   long long ffsz[3] = {};
   long long ffoff[24] = {};
   void* ex0b = nullptr;
@@ -301,6 +302,7 @@ FarField dev_ff(const fdtd_ctx* c) {
   ff.acc = c->acc;
   for (int a = 0; a < 24; a++) ff.off[a] = c->ffoff[a];
   for (int a = 0; a < 3; a++) ff.sz[a] = c->ffsz[a];
+  ff.kahan = c->acc_kahan;
   return ff;
 }
 
@@ -1144,6 +1146,25 @@ int fdtd_ctx_read_farfield(fdtd_ctx* c, int array, double* re, double* im, long 
   CK(cudaSetDevice(c->device));
   CK(xfer(c, re, c->acc + c->ffoff[array], m * sizeof(double), cudaMemcpyDeviceToHost));
   CK(xfer(c, im, c->acc + c->ffoff[array] + m, m * sizeof(double), cudaMemcpyDeviceToHost));
+  if (c->acc_kahan) {
+    // each 8-byte slot holds (sum, compensation) as two floats; the sum is sum - compensation
+    for (double* a : {re, im})
+      for (long long q = 0; q < m; q++) {
+        float v[2];
+        memcpy(v, &a[q], sizeof(v));
+        a[q] = (double)v[0] - (double)v[1];
+      }
+  }
+  return FDTD_OK;
+}
+
+int fdtd_ctx_set_dft_accumulator(fdtd_ctx* c, int kahan_fp32) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (kahan_fp32 != 0 && kahan_fp32 != 1) return fail(FDTD_ERR_BADARG, "accumulator mode %d not in {0,1}", kahan_fp32);
+  if (kahan_fp32 && c->prec == FDTD_PREC_F64) return fail(FDTD_ERR_BADARG, "FP64 problems keep FP64 accumulators");
+  if (c->ts != 0) return fail(FDTD_ERR_STATE, "the accumulator mode is set before the first step");
+  c->acc_kahan = kahan_fp32;
+  invalidate(c);
   return FDTD_OK;
 }
 
@@ -1207,6 +1228,13 @@ int fdtd_ctx_farfield_post(fdtd_ctx* c, const double* theta, const double* phi, 
   CK(cudaSetDevice(c->device));
   FFPost P{};
   P.acc = c->acc;
+  double* conv = nullptr;
+  if (c->acc_kahan) {
+    const long long n = c->ffoff[23] + 2LL * c->nFreq * c->ffsz[2];
+    if (cudaMalloc(&conv, n * sizeof(double)) != cudaSuccess) return fail(FDTD_ERR_OOM, "far-field post buffer");
+    k_kahan_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->acc, conv, n);
+    P.acc = conv;
+  }
   for (int a = 0; a < 24; a++) P.off[a] = c->ffoff[a];
   for (int a = 0; a < 3; a++) P.sz[a] = c->ffsz[a];
   P.nFreq = c->nFreq;
@@ -1262,6 +1290,7 @@ int fdtd_ctx_farfield_post(fdtd_ctx* c, const double* theta, const double* phi, 
   cudaFree(dradp);
   cudaFree(dang);
   cudaFree(dout);
+  cudaFree(conv);
   return rc;
 }
 

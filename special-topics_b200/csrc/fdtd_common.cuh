@@ -76,6 +76,7 @@ struct FarField {
   double* acc;                 // 24 arrays, each re[nFreq][sz] then im[nFreq][sz]
   long long off[24];
   long long sz[3];             // x-, y-, z-face point counts
+  int kahan;                   // accumulators are FP32 (sum, compensation) pairs, not FP64
 };
 
 // Lumped source on the cell this thread owns (sources.js:271-288).
@@ -129,9 +130,25 @@ enum {
   CMYXP, CMZXP, CMYXN, CMZXN, CMXYP, CMZYP, CMXYN, CMZYN, CMXZP, CMYZP, CMXZN, CMYZN
 };
 
+// One Kahan-compensated FP32 step: v = (sum, compensation), sum += x.
+__device__ __forceinline__ void kahan_add(float2* v, float x) {
+  float2 a = *v;
+  const float y = __fsub_rn(x, a.y);
+  const float t = __fadd_rn(a.x, y);
+  a.y = __fsub_rn(__fsub_rn(t, a.x), y);
+  a.x = t;
+  *v = a;
+}
+
 __device__ __forceinline__ void acc2(const FarField& ff, int a, long long p, double c, double s, double t) {
   double* re = ff.acc + ff.off[a] + p;
   double* im = re + ff.nFreq * ff.sz[(a % 12) / 4];
+  if (ff.kahan) {
+    const float tf = (float)t;
+    kahan_add(reinterpret_cast<float2*>(re), __fmul_rn((float)c, tf));
+    kahan_add(reinterpret_cast<float2*>(im), __fmul_rn((float)s, tf));
+    return;
+  }
   *re = add(*re, mul(c, t));
   *im = add(*im, mul(s, t));
 }
@@ -224,8 +241,11 @@ __device__ __forceinline__ void epilogue_thread(const Fields<T>& f, const GridDi
       acc2(ff, CMXZP, p, ce, se, tmxzp);
       acc2(ff, CMYZP, p, ce, se, tmyzp);
       // zp Jx: the reference adds the Hx average, then swaps it for the Hy
-      // average in a second statement (farfield.js:211-225); keep both roundings.
-      {
+      // average in a second statement (farfield.js:211-225); keep both roundings
+      // (with compensated FP32 accumulators only the net Hy term is added).
+      if (ff.kahan) {
+        acc2(ff, CJXZP, p, ch, sh, tjxzp2);
+      } else {
         double* re = ff.acc + ff.off[CJXZP] + p;
         double* im = re + ff.nFreq * ff.sz[2];
         const double r1 = add(*re, mul(ch, tjxzp));

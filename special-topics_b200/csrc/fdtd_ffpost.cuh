@@ -46,6 +46,14 @@ __device__ __forceinline__ void face_arrays(int f, int& j1, int& j2, int& m1, in
   m2 = tab[f][3];
 }
 
+// Compensated FP32 accumulator pairs (sum, compensation) -> FP64 values.
+__global__ void k_kahan_to_f64(const double* __restrict__ acc, double* __restrict__ out, long long n) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float2 v = reinterpret_cast<const float2*>(acc)[q];
+  out[q] = (double)v.x - (double)v.y;
+}
+
 // Radiated power of every frequency: block f, fixed-order reduction.
 __global__ void __launch_bounds__(256) k_ff_power(FFPost P, double* __restrict__ radp) {
   __shared__ double red[256];

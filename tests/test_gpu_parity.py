@@ -260,3 +260,22 @@ def test_device_farfield_post_matches_host(name):
         assert np.allclose(radp, radp_h, rtol=1e-10, atol=0)
         for d, h in ((dth, dth_h), (dph, dph_h)):
             assert np.abs(d - h).max() <= 1e-9 * np.abs(h).max()
+
+
+def test_kahan_fp32_accumulators_track_fp64_ones():
+    scn, steps = CASES["small-xp"]()
+    p = build_problem_from_scenario(scn, steps, per_cell=False)
+    with Engine(p, "f32-table") as a, Engine(p, "f32-table", dft_accumulator="kahan-f32") as b:
+        a.run(steps)
+        b.run(steps)
+        fa, fb = a.farfield(), b.farfield()
+        for name in FF_NAMES:
+            for q in range(2):
+                scale = np.abs(fa[name][q]).max() + 1e-30
+                assert np.abs(fa[name][q] - fb[name][q]).max() <= 1e-5 * scale, name
+        ra, _, _ = a.farfield_post(np.zeros(1), np.zeros(1))
+        rb, _, _ = b.farfield_post(np.zeros(1), np.zeros(1))
+        assert np.allclose(ra, rb, rtol=1e-4)
+    with Engine(build_problem_from_scenario(scn, steps), "f64") as c:
+        with pytest.raises(N.FdtdError):
+            N.check(N.lib().fdtd_ctx_set_dft_accumulator(c._h, 1))
