@@ -18,6 +18,11 @@ CACHE = os.path.join(N.BUILD_DIR, "tiling_cache.json")
 CHUNKS = (1, 2, 4, 8, 16, 32, 64)
 ROWS = (2, 4, 8)
 PREFETCH = (1, 2)
+TABLE_PREFETCH = (1, 2, 3, 4)   # 3, 4: shared-memory stages, material-table problems only
+
+
+def prefetch_depths(precision: str) -> tuple:
+    return TABLE_PREFETCH if precision == "f32-table" else PREFETCH
 
 
 def _key(problem, precision: str) -> str:
@@ -51,7 +56,8 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
     cache = _load()
     if use_cache and key in cache:
         return cache[key]
-    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS) * len(PREFETCH)) + 8
+    depths = prefetch_depths(precision)
+    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS) * len(depths)) + 8
     if problem.grid.numberOfTimeSteps < need:
         raise ValueError(f"the scratch problem needs at least {need} time steps for tuning")
     nx = problem.grid.nx
@@ -62,7 +68,7 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
             if chunk > nx + 1:
                 continue
             for rows in ROWS:
-                for pf in PREFETCH:
+                for pf in depths:
                     set_tiling(eng, chunk, rows, pf)
                     eng.run_timed(steps_per_candidate)          # capture and warm the graph
                     ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
@@ -90,8 +96,9 @@ def batch_key(batch) -> str:
     return f"batch:{batch.engines[0].precision}:{len(dims)}:{lo[0]}x{lo[1]}x{lo[2]}-{hi[0]}x{hi[1]}x{hi[2]}"
 
 
-def batch_steps_needed(steps_per_candidate: int) -> int:
-    return 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(PREFETCH) + len(BATCH_GROUPS))
+def batch_steps_needed(steps_per_candidate: int, precision: str = "f32-table") -> int:
+    return 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(prefetch_depths(precision))
+                                      + len(BATCH_GROUPS))
 
 
 def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> dict:
@@ -117,7 +124,7 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
 
     for chunk in BATCH_CHUNKS:
         for rows in ROWS:
-            for pf in PREFETCH:
+            for pf in prefetch_depths(batch.engines[0].precision):
                 trial(min(chunk, max_x), rows, pf, 0)
     best = min(table, key=lambda r: r["ms_per_step"])
     for group in BATCH_GROUPS[1:]:

@@ -370,6 +370,28 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   return p;
 }
 
+// Step kernels for a prefetch depth: 1, 2 = planes prefetched in registers;
+// 3, 4 = planes staged through shared memory (material-table problems only).
+template <typename T, class C, bool EXACT>
+void (*step_kernel(bool electric, int pf))(StepParams<T, C>) {
+  if constexpr (C::kTable) {
+    if (pf == 3) return electric ? k_step_e<T, C, EXACT, 3> : k_step_h<T, C, EXACT, 3>;
+    if (pf == 4) return electric ? k_step_e<T, C, EXACT, 4> : k_step_h<T, C, EXACT, 4>;
+  }
+  if (pf == 2) return electric ? k_step_e<T, C, EXACT, 2> : k_step_h<T, C, EXACT, 2>;
+  return electric ? k_step_e<T, C, EXACT, 1> : k_step_h<T, C, EXACT, 1>;
+}
+
+// Dynamic shared memory of a step launch; raises the kernel's limit when the
+// stages need more than the default 48 KB.
+template <class K>
+int stage_smem(K kernel, int pf, int threads, size_t* bytes) {
+  *bytes = pf >= 3 ? (size_t)stage_smem_bytes(pf, threads) : 0;
+  if (*bytes > 48 * 1024)
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes));
+  return FDTD_OK;
+}
+
 // Per-kernel timing of a profiled run: events around each launch.
 struct KernelTimer {
   cudaEvent_t ev[5];
@@ -391,19 +413,19 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   const unsigned mid_blocks = (unsigned)((plane + pr.n_i + 255) / 256);
   const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
   const unsigned epi_blocks = (unsigned)((nff + pr.n_v + 255) / 256);
+  auto kh = step_kernel<T, C, EXACT>(false, c->prefetch);
+  auto ke = step_kernel<T, C, EXACT>(true, c->prefetch);
+  size_t smem = 0;
+  int rc = stage_smem(kh, c->prefetch, 32 * c->block_rows, &smem);
+  if (!rc) rc = stage_smem(ke, c->prefetch, 32 * c->block_rows, &smem);
+  if (rc) return rc;
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], c->stream));
-    if (c->prefetch == 2)
-      k_step_h<T, C, EXACT, 2><<<grd, blk, 0, c->stream>>>(p);
-    else
-      k_step_h<T, C, EXACT, 1><<<grd, blk, 0, c->stream>>>(p);
+    kh<<<grd, blk, smem, c->stream>>>(p);
     if (tm) CK(cudaEventRecord(tm->ev[1], c->stream));
     k_step_mid<T, C, EXACT><<<mid_blocks, 256, 0, c->stream>>>(p, pr);
     if (tm) CK(cudaEventRecord(tm->ev[2], c->stream));
-    if (c->prefetch == 2)
-      k_step_e<T, C, EXACT, 2><<<grd, blk, 0, c->stream>>>(p);
-    else
-      k_step_e<T, C, EXACT, 1><<<grd, blk, 0, c->stream>>>(p);
+    ke<<<grd, blk, smem, c->stream>>>(p);
     if (tm) CK(cudaEventRecord(tm->ev[3], c->stream));
     if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, c->stream>>>(p.f, p.g, ff, pr, c->d_ts);
     if (tm) {
@@ -631,7 +653,8 @@ int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
     for (int q = 0; q < 18 && !rc; q++) rc = dalloc(c, &c->coef[q], coef_count(c, q) * c->esz);
   }
   if (!rc && c->prec == FDTD_PREC_F32_TABLE) {
-    for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6]);
+    // 4 bytes of padding: the staged kernels copy whole aligned words of ids
+    for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6] + 4);
   }
   if (!rc) rc = ensure_traces(c);
   if (!rc) {
@@ -1056,7 +1079,9 @@ int fdtd_ctx_run(fdtd_ctx* c, int count) {
 
 int fdtd_ctx_set_prefetch(fdtd_ctx* c, int planes) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
-  if (planes != 1 && planes != 2) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in {1,2}", planes);
+  if (planes < 1 || planes > 4) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in 1..4", planes);
+  if (planes > 2 && c->prec != FDTD_PREC_F32_TABLE)
+    return fail(FDTD_ERR_BADARG, "prefetch depths 3 and 4 (shared-memory stages) need a material-table problem");
   c->prefetch = planes;
   invalidate(c);
   return FDTD_OK;
@@ -1392,6 +1417,22 @@ int upload_vec(fdtd_batch* b, V** dst, const std::vector<V>& v) {
   return FDTD_OK;
 }
 
+// Batched H/E kernel for a prefetch depth (as step_kernel) and grid kind.
+template <typename T, class C, bool EXACT>
+void (*batch_kernel(bool electric, int pf, bool persist))(const Instance<T, C>*, const BatchTile*, int, BatchCtl*,
+                                                           int) {
+#define FDTD_BK(PF)                                                                                           \
+  (electric ? (persist ? k_batch_half<T, C, EXACT, PF, true, true> : k_batch_half<T, C, EXACT, PF, true, false>) \
+            : (persist ? k_batch_half<T, C, EXACT, PF, false, true> : k_batch_half<T, C, EXACT, PF, false, false>))
+  if constexpr (C::kTable) {
+    if (pf == 3) return FDTD_BK(3);
+    if (pf == 4) return FDTD_BK(4);
+  }
+  if (pf == 2) return FDTD_BK(2);
+  return FDTD_BK(1);
+#undef FDTD_BK
+}
+
 // The parameter blocks of every member (member state may have moved since the
 // last run: traces, tables) and, when the work lists changed, the lists.
 template <typename T, class C, bool EXACT>
@@ -1452,13 +1493,14 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
   int sms = 0, per_h = 0, per_e = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
   const int threads = 32 * b->block_rows;
-  if (b->prefetch == 2) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_h, k_batch_half<T, C, EXACT, 2, false, true>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_e, k_batch_half<T, C, EXACT, 2, true, true>, threads, 0));
-  } else {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_h, k_batch_half<T, C, EXACT, 1, false, true>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_e, k_batch_half<T, C, EXACT, 1, true, true>, threads, 0));
-  }
+  size_t smem = 0;
+  auto kh = batch_kernel<T, C, EXACT>(false, b->prefetch, true);
+  auto ke = batch_kernel<T, C, EXACT>(true, b->prefetch, true);
+  int rc = stage_smem(kh, b->prefetch, threads, &smem);
+  if (!rc) rc = stage_smem(ke, b->prefetch, threads, &smem);
+  if (rc) return rc;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_h, kh, threads, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_e, ke, threads, smem));
   b->grid_h = std::max(1, per_h) * sms;
   b->grid_e = std::max(1, per_e) * sms;
   return FDTD_OK;
@@ -1471,20 +1513,19 @@ int batch_enqueue(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
   const dim3 blk(32, b->block_rows);
   const unsigned gh = b->group ? (unsigned)std::min(b->grid_h, (nt + b->group - 1) / b->group) : (unsigned)nt;
   const unsigned ge = b->group ? (unsigned)std::min(b->grid_e, (nt + b->group - 1) / b->group) : (unsigned)nt;
-  // kernel for (prefetch, electric, persistent)
-  using K = void (*)(const Instance<T, C>*, const BatchTile*, int, BatchCtl*, int);
-  const K kern[2][2][2] = {{{k_batch_half<T, C, EXACT, 1, false, false>, k_batch_half<T, C, EXACT, 1, false, true>},
-                            {k_batch_half<T, C, EXACT, 1, true, false>, k_batch_half<T, C, EXACT, 1, true, true>}},
-                           {{k_batch_half<T, C, EXACT, 2, false, false>, k_batch_half<T, C, EXACT, 2, false, true>},
-                            {k_batch_half<T, C, EXACT, 2, true, false>, k_batch_half<T, C, EXACT, 2, true, true>}}};
-  const int pf = b->prefetch == 2 ? 1 : 0, ps = b->group ? 1 : 0;
+  auto kh = batch_kernel<T, C, EXACT>(false, b->prefetch, b->group != 0);
+  auto ke = batch_kernel<T, C, EXACT>(true, b->prefetch, b->group != 0);
+  size_t smem = 0;
+  int rc = stage_smem(kh, b->prefetch, 32 * b->block_rows, &smem);
+  if (!rc) rc = stage_smem(ke, b->prefetch, 32 * b->block_rows, &smem);
+  if (rc) return rc;
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], b->stream));
-    kern[pf][0][ps]<<<gh, blk, 0, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    kh<<<gh, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
     if (tm) CK(cudaEventRecord(tm->ev[1], b->stream));
     k_batch_mid<T, C, EXACT><<<(unsigned)b->mid.size(), 256, 0, b->stream>>>(in, b->d_mid, b->d_ctl);
     if (tm) CK(cudaEventRecord(tm->ev[2], b->stream));
-    kern[pf][1][ps]<<<ge, blk, 0, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    ke<<<ge, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
     if (tm) CK(cudaEventRecord(tm->ev[3], b->stream));
     if (!b->epi.empty()) k_batch_epilogue<T, C><<<(unsigned)b->epi.size(), 256, 0, b->stream>>>(in, b->d_epi);
     if (tm) {
@@ -1646,7 +1687,9 @@ int fdtd_batch_set_tiling(fdtd_batch* b, int x_planes_per_thread, int block_rows
     return fail(FDTD_ERR_BADARG, "x planes per thread %d outside 1..1024", x_planes_per_thread);
   if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8)
     return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8}", block_rows);
-  if (prefetch != 1 && prefetch != 2) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in {1,2}", prefetch);
+  if (prefetch < 1 || prefetch > 4) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in 1..4", prefetch);
+  if (prefetch > 2 && b->prec != FDTD_PREC_F32_TABLE)
+    return fail(FDTD_ERR_BADARG, "prefetch depths 3 and 4 (shared-memory stages) need material-table members");
   if (group < 0 || group > 4096) return fail(FDTD_ERR_BADARG, "tile group %d outside 0..4096", group);
   if (b->ichunk != x_planes_per_thread || b->block_rows != block_rows || b->prefetch != prefetch ||
       b->group != group)

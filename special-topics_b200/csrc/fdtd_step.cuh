@@ -553,11 +553,122 @@ struct BandForm {
   static constexpr bool kPrefetch = false;
 };
 
+// ---------------------------------------------------------------------------
+// Interior planes staged through shared memory (material-table problems,
+// prefetch depth S = 3 or 4): each thread copies its own column's inputs of
+// the next S planes into private shared-memory slots with cp.async, so S
+// planes of loads are in flight without holding registers.  A plane's words
+// are then read back into an HIn / EIn and go through h_store / e_store, so
+// the arithmetic is that of the register-prefetched form.
+// ---------------------------------------------------------------------------
+extern __shared__ float fdtd_stage_smem[];
+
+__device__ __forceinline__ void cp4(float* dst, const void* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The 4-byte word holding id `idx` of a uint8 id array (the arrays are
+// 4-byte aligned and padded by 4 bytes), and the id's byte in that word.
+__device__ __forceinline__ const void* id_word(const unsigned char* ids, int idx) { return ids + (idx & ~3); }
+__device__ __forceinline__ unsigned char id_of(float w, int idx) {
+  return (unsigned char)(__float_as_uint(w) >> (8 * (idx & 3)));
+}
+
+constexpr int kStageWords = 13;  // words staged per plane of an H or E column
+
+// Word v of a thread's plane slot lives at s[v * nthr]: consecutive threads
+// use consecutive words, so the slots are free of bank conflicts.
+__device__ __forceinline__ void h_stage(const StepParams<float, TableCoef>& p, const HCol<float>& c, int i, float* s,
+                                        int nthr) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<float>& f = p.f;
+  const int ex = i * sEx + c.ob;
+  cp4(s, f.Ex + ex);
+  if (c.hx_ok) {
+    const int idx = i * sHx + c.oa;
+    cp4(s + 1 * nthr, f.Hx + idx);
+    cp4(s + 2 * nthr, f.Ey + i * sHzEy + c.ob + 1);
+    cp4(s + 3 * nthr, f.Ez + i * sHyEz + c.oa + nz);
+    cp4(s + 4 * nthr, id_word(p.coef.ids[0], idx));
+  }
+  if (c.hy_ok) {
+    const int idx = i * sHyEz + c.oa;
+    cp4(s + 5 * nthr, f.Hy + idx);
+    cp4(s + 6 * nthr, f.Ex + ex + 1);
+    cp4(s + 7 * nthr, f.Ez + idx + sHyEz);
+    cp4(s + 8 * nthr, id_word(p.coef.ids[1], idx));
+  }
+  if (c.hz_ok) {
+    const int idx = i * sHzEy + c.ob;
+    cp4(s + 9 * nthr, f.Hz + idx);
+    cp4(s + 10 * nthr, f.Ex + ex + nzp1);
+    cp4(s + 11 * nthr, f.Ey + idx + sHzEy);
+    cp4(s + 12 * nthr, id_word(p.coef.ids[2], idx));
+  }
+}
+
+__device__ __forceinline__ void h_unstage(const StepParams<float, TableCoef>& p, const HCol<float>& c, int i,
+                                          const float* s, int nthr, HIn<float, TableCoef>& in) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  in.ex = s[0];
+  if (c.hx_ok) {
+    in.hx = s[1 * nthr];
+    in.ey_kp = s[2 * nthr];
+    in.ez_jp = s[3 * nthr];
+    in.r0 = id_of(s[4 * nthr], i * ny * nz + c.oa);
+  }
+  if (c.hy_ok) {
+    in.hy = s[5 * nthr];
+    in.ex_kp = s[6 * nthr];
+    in.ez_n = s[7 * nthr];
+    in.r1 = id_of(s[8 * nthr], i * nyp1 * nz + c.oa);
+  }
+  if (c.hz_ok) {
+    in.hz = s[9 * nthr];
+    in.ex_jp = s[10 * nthr];
+    in.ey_n = s[11 * nthr];
+    in.r2 = id_of(s[12 * nthr], i * ny * nzp1 + c.ob);
+  }
+}
+
+// Planes [xa, xb) of an H column with S planes of loads in flight.
+template <int S>
+__device__ __forceinline__ void h_staged_range(const StepParams<float, TableCoef>& p, const HCol<float>& c, int xa,
+                                               int xb, float& ez_c, float& ey_c) {
+  const int nthr = blockDim.x * blockDim.y;
+  float* base = fdtd_stage_smem + threadIdx.y * blockDim.x + threadIdx.x;
+  const int n = xb - xa;
+  for (int q = 0; q < S; q++) {
+    if (q < n) h_stage(p, c, xa + q, base + q * kStageWords * nthr, nthr);
+    cp_commit();
+  }
+  for (int q = 0; q < n; q++) {
+    float* slot = base + (q % S) * kStageWords * nthr;
+    cp_wait<S - 1>();
+    HIn<float, TableCoef> in;
+    h_unstage(p, c, xa + q, slot, nthr, in);
+    h_store<float, TableCoef, false>(p, c, xa + q, in, ez_c, ey_c);
+    if (q + S < n) h_stage(p, c, xa + q + S, slot, nthr);
+    cp_commit();
+  }
+}
+
+// Bytes of dynamic shared memory the staged form needs for a block.
+__host__ __device__ constexpr int stage_smem_bytes(int S, int threads) { return S * kStageWords * threads * 4; }
+
 // Minimum resident 256-thread blocks per SM the register budget is fitted to:
-// FP64 values need twice the registers; a deeper prefetch holds one more plane.
+// FP64 values need twice the registers; a deeper register prefetch holds one
+// more plane; the shared-memory stages (PF 3, 4) hold theirs outside registers.
 template <typename T, int PF>
 struct MinBlocks {
-  static constexpr int value = sizeof(T) == 8 ? 2 : (PF == 1 ? 4 : 3);
+  static constexpr int value = sizeof(T) == 8 ? 2 : (PF == 2 ? 3 : 4);
 };
 
 // H update of one tile: columns (bx*32 + tx, by*rows + ty), x planes from
@@ -610,8 +721,9 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
   } else {
     for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
   }
-  if (xa < xb) {
-    // software pipeline: plane i+1's loads are in flight while plane i is computed and stored
+  if constexpr (PF >= 3 && C::kTable) {
+    h_staged_range<PF>(p, c, xa, xb, ez_c, ey_c);
+  } else if (xa < xb) {
     // software pipeline: the loads of the next PF planes are in flight while
     // plane i is computed and stored
     HIn<T, C> cur, nxt, nx2;
@@ -795,6 +907,59 @@ __device__ __forceinline__ void e_load(const StepParams<T, C>& p, const ECol<T>&
     in.ez = f.Ez[idx];
     in.hx_jm = f.Hx[i * sHx + c.oa - nz];
     in.r2 = p.coef.fetch(5, idx);
+  }
+}
+
+__device__ __forceinline__ void e_stage(const StepParams<float, TableCoef>& p, const ECol<float>& c, int i, float* s,
+                                        int nthr) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<float>& f = p.f;
+  if (c.jy && c.kz) {
+    const int idx = i * sEx + c.ob;
+    cp4(s, f.Ex + idx);
+    cp4(s + 1 * nthr, id_word(p.coef.ids[3], idx));
+  }
+  if (c.ey_ok) cp4(s + 2 * nthr, f.Hz + i * sHzEy + c.ob);
+  if (c.ez_ok) cp4(s + 3 * nthr, f.Hy + i * sHyEz + c.oa);
+  if (c.jy) cp4(s + 4 * nthr, f.Hz + i * sHzEy + c.ob - nzp1);
+  if (c.kz) cp4(s + 5 * nthr, f.Hy + i * sHyEz + c.oa - 1);
+  if (c.ey_ok && c.ez_ok) cp4(s + 6 * nthr, f.Hx + i * sHx + c.oa);
+  if (c.kz && c.ey_ok) {
+    const int idx = i * sHzEy + c.ob;
+    cp4(s + 7 * nthr, f.Ey + idx);
+    cp4(s + 8 * nthr, f.Hx + i * sHx + c.oa - 1);
+    cp4(s + 9 * nthr, id_word(p.coef.ids[4], idx));
+  }
+  if (c.jy && c.ez_ok) {
+    const int idx = i * sHyEz + c.oa;
+    cp4(s + 10 * nthr, f.Ez + idx);
+    cp4(s + 11 * nthr, f.Hx + i * sHx + c.oa - nz);
+    cp4(s + 12 * nthr, id_word(p.coef.ids[5], idx));
+  }
+}
+
+__device__ __forceinline__ void e_unstage(const StepParams<float, TableCoef>& p, const ECol<float>& c, int i,
+                                          const float* s, int nthr, EIn<float, TableCoef>& in) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  if (c.jy && c.kz) {
+    in.ex = s[0];
+    in.r0 = id_of(s[1 * nthr], i * nyp1 * nzp1 + c.ob);
+  }
+  if (c.ey_ok) in.hz = s[2 * nthr];
+  if (c.ez_ok) in.hy = s[3 * nthr];
+  if (c.jy) in.hz_jm = s[4 * nthr];
+  if (c.kz) in.hy_km = s[5 * nthr];
+  if (c.ey_ok && c.ez_ok) in.hx = s[6 * nthr];
+  if (c.kz && c.ey_ok) {
+    in.ey = s[7 * nthr];
+    in.hx_km = s[8 * nthr];
+    in.r1 = id_of(s[9 * nthr], i * ny * nzp1 + c.ob);
+  }
+  if (c.jy && c.ez_ok) {
+    in.ez = s[10 * nthr];
+    in.hx_jm = s[11 * nthr];
+    in.r2 = id_of(s[12 * nthr], i * nyp1 * nz + c.oa);
   }
 }
 
@@ -995,6 +1160,28 @@ __device__ __forceinline__ void e_band_range(const StepParams<T, C>& p, const EC
   }
 }
 
+// Planes [xa, xb) of an E column with S planes of loads in flight.
+template <int S>
+__device__ __forceinline__ void e_staged_range(const StepParams<float, TableCoef>& p, const ECol<float>& c, int xa,
+                                               int xb, float& hz_p, float& hy_p) {
+  const int nthr = blockDim.x * blockDim.y;
+  float* base = fdtd_stage_smem + threadIdx.y * blockDim.x + threadIdx.x;
+  const int n = xb - xa;
+  for (int q = 0; q < S; q++) {
+    if (q < n) e_stage(p, c, xa + q, base + q * kStageWords * nthr, nthr);
+    cp_commit();
+  }
+  for (int q = 0; q < n; q++) {
+    float* slot = base + (q % S) * kStageWords * nthr;
+    cp_wait<S - 1>();
+    EIn<float, TableCoef> in;
+    e_unstage(p, c, xa + q, slot, nthr, in);
+    e_store<float, TableCoef, false>(p, c, xa + q, in, hz_p, hy_p);
+    if (q + S < n) e_stage(p, c, xa + q + S, slot, nthr);
+    cp_commit();
+  }
+}
+
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
   const int k = bx * blockDim.x + threadIdx.x;
@@ -1046,7 +1233,9 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
   } else {
     for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
   }
-  if (xa < xb) {
+  if constexpr (PF >= 3 && C::kTable) {
+    e_staged_range<PF>(p, c, xa, xb, hz_p, hy_p);
+  } else if (xa < xb) {
     EIn<T, C> cur, nxt, nx2;
     e_load(p, c, xa, cur);
     if (PF == 2 && xa + 1 < xb) e_load(p, c, xa + 1, nxt);

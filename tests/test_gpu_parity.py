@@ -236,7 +236,7 @@ def test_autotuner_picks_a_measured_shape(tmp_path, monkeypatch):
     from special_topics_b200 import autotune
     monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tiling.json"))
     scn, _ = CASES["small-xp"]()
-    p = build_problem_from_scenario(scn, 800)
+    p = build_problem_from_scenario(scn, 1400)
     res = autotune.tune(p, "f32-table", steps_per_candidate=8)
     assert {"chunk", "rows", "ms_per_step"} <= set(res)
     assert res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
@@ -279,3 +279,23 @@ def test_kahan_fp32_accumulators_track_fp64_ones():
     with Engine(build_problem_from_scenario(scn, steps), "f64") as c:
         with pytest.raises(N.FdtdError):
             N.check(N.lib().fdtd_ctx_set_dft_accumulator(c._h, 1))
+
+
+@pytest.mark.parametrize("chunk,rows,pf", [(5, 2, 3), (16, 8, 4), (1, 4, 4), (64, 2, 3), (3, 8, 2)])
+def test_shared_memory_stages_give_identical_table_results(chunk, rows, pf):
+    """Prefetch depths 3 and 4 stage the interior planes through shared
+    memory; material-table results are bit-identical to the depth-1 form."""
+    from special_topics_b200 import autotune
+    scn, steps = CASES["ifa-fr4-substrate"]()
+    p = build_problem_from_scenario(scn, steps, per_cell=False)
+    with Engine(p, "f32-table") as a, Engine(p, "f32-table") as b:
+        autotune.set_tiling(a, 8, 4, 1)
+        autotune.set_tiling(b, min(chunk, p.grid.nx + 1), rows, pf)
+        a.run(steps)
+        b.run(steps)
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        for fld in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"):
+            assert np.array_equal(a.field(fld), b.field(fld)), fld
+    with Engine(build_problem_from_scenario(scn, steps), "f64") as c:
+        with pytest.raises(N.FdtdError):
+            autotune.set_tiling(c, 8, 4, 3)
