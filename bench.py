@@ -178,6 +178,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--tiling", default=None, help="fixed launch shape chunk,rows,prefetch (skips the tuner)")
     ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
@@ -244,12 +245,26 @@ def main():
     setup_s = time.perf_counter() - t0
     cells = prob.grid.cells
 
+    # --- launch shape from the autotuner (timed on a scratch copy of the problem)
+    from special_topics_b200 import autotune
+    tuning = None
+    if args.tiling:
+        ch, rw, pf = (int(x) for x in args.tiling.split(","))
+        tuning = {"chunk": ch, "rows": rw, "prefetch": pf, "ms_per_step": None}
+    elif not args.no_tune:
+        scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000), 3000,
+                                              per_cell=(args.precision != "f32-table"))
+        tuning = autotune.tune(scratch, args.precision, device=local, steps_per_candidate=args.tune_steps)
+        del scratch
+
     # --- end to end through the C ABI with host buffers: upload + K steps + readback
     barrier()
     e2e = None
     t0 = time.perf_counter()
     if not args.no_e2e:
         eng = Engine(prob, args.precision, device=local)
+        if tuning:
+            autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
         h2d = _uploaded_bytes(prob, args.precision)
         eng.run(K)
         V, I = eng.voltages(K), eng.currents(K)
@@ -262,15 +277,6 @@ def main():
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                "note": "one step's share of a whole run through the C ABI: uploads from host buffers, "
                        "K steps, readback of port traces and far-field accumulators"}
-
-    # --- launch shape from the autotuner (timed on a scratch copy of the problem)
-    from special_topics_b200 import autotune
-    tuning = None
-    if not args.no_tune:
-        scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000), 3000,
-                                              per_cell=(args.precision != "f32-table"))
-        tuning = autotune.tune(scratch, args.precision, device=local, steps_per_candidate=args.tune_steps)
-        del scratch
 
     # --- device-timed run
     eng = Engine(prob, args.precision, device=local)
