@@ -288,7 +288,9 @@ def _variant_problem(args):
 
 
 def variant_problems(seeds, steps: int, pool=None) -> list:
-    """Problems of the inverted-F variant family (workloads.ifa_variant)."""
+    """Problems of the inverted-F variant family (workloads.ifa_variant).
+    A process pool must make this package importable in its workers first
+    (an initializer that loads it), or the workers cannot run the jobs."""
     jobs = [(int(s), steps) for s in seeds]
     return pool.map(_variant_problem, jobs) if pool is not None else [_variant_problem(j) for j in jobs]
 

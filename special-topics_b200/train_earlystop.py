@@ -71,10 +71,9 @@ def build_set(ES, pool, seeds, steps, policy, tiling):
     return np.array(x, np.float32), np.array(y, np.float32), keep, dev_s
 
 
-def evaluate(ES, pool, seeds, net, policy, tiling, group=128):
-    """Plain FP64 reference vs the early-stopped FP32 runs (with and without the network)."""
+def plain_reference(ES, probs, policy, tiling, group=128):
+    """S11 of plain FP64 batched runs of the full step count, and their wall time."""
     from special_topics_b200.backend import Batch, Engine
-    probs = ES.variant_problems(seeds, policy.n_total, pool)
     freqs = ES.S11_FREQS
     ref, t_plain = [], 0.0
     for g0 in range(0, len(probs), group):
@@ -91,6 +90,13 @@ def evaluate(ES, pool, seeds, net, policy, tiling, group=128):
         finally:
             for e in engs:
                 e.close()
+    return np.array(ref), t_plain
+
+
+def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128):
+    """Plain FP64 reference vs the early-stopped FP32 runs (with and without the network)."""
+    from special_topics_b200.backend import Engine
+    freqs = ES.S11_FREQS
     out = {"plain_f64": {"time_s": t_plain, "steps": policy.n_total * len(probs)}}
     for name, use_net in (("learned", True), ("no_network", False)):
         errs, stops, t = [], [], 0.0
@@ -127,18 +133,29 @@ def main():
     ap.add_argument("--n-check", type=int, default=300)
     ap.add_argument("--max-resid", type=float, default=0.03)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cache", default=None, help="npz of a previous run's training set and test reference")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
-    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
+    # workers register the package under its import name before any task arrives
+    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1), initializer=_package)
     _package()
     from special_topics_b200 import earlystop as ES
     policy = ES.StopPolicy(n_check=args.n_check, max_resid=args.max_resid)
     tiling = dict(chunk=16, rows=4, prefetch=1, group=0)
     metrics = {"policy": policy.__dict__, "arch": ES.ARCH}
     t0 = time.perf_counter()
-    x, y, keep, dev_s = build_set(ES, pool, range(1000, 1000 + args.train), policy.n_total, policy, tiling)
-    metrics["train_set"] = {"runs": args.train, "labelled": len(keep), "solver_device_s": dev_s,
-                            "wall_s": time.perf_counter() - t0}
+    test_seeds = range(10000, 10000 + args.test)
+    test_probs = ES.variant_problems(test_seeds, policy.n_total, pool)
+    if args.cache and os.path.exists(args.cache):
+        z = np.load(args.cache)
+        x, y, ref, t_plain = z["x"], z["y"], z["ref"], float(z["t_plain"])
+        metrics["train_set"] = {"runs": args.train, "labelled": len(x), "from_cache": True}
+    else:
+        x, y, keep, dev_s = build_set(ES, pool, range(1000, 1000 + args.train), policy.n_total, policy, tiling)
+        metrics["train_set"] = {"runs": args.train, "labelled": len(keep), "solver_device_s": dev_s,
+                                "wall_s": time.perf_counter() - t0}
+        ref, t_plain = plain_reference(ES, test_probs, policy, tiling)
+        np.savez(os.path.join(args.out, "es_data.npz"), x=x, y=y, ref=ref, t_plain=t_plain)
     # target scaling: each output standardised over the training set
     mu, sd = y.mean(axis=0), y.std(axis=0) + 1e-6
     yn = (y - mu) / sd
@@ -161,7 +178,7 @@ def main():
                                "alpha_rel_median": float(np.median(np.abs(np.exp(pv[:, 1] - y[:n_val, 1]) - 1)))}
     net.out_mu, net.out_sd = mu.astype(np.float32), sd.astype(np.float32)
     net.save(os.path.join(args.out, "es_weights.npz"))
-    metrics["evaluation"] = evaluate(ES, pool, range(10000, 10000 + args.test), net, policy, tiling)
+    metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling)
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
     print(json.dumps(metrics["evaluation"]), flush=True)
