@@ -30,6 +30,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "Gcell-updates/s & time-to-S11 at 0.1 dB: FP32/learned vs FP64 plain, 1 B200"
 FALLBACK_HBM_GBS = 6650.0
+NOMINAL_HBM_GBS = 8000.0   # the B200 HBM3e figure the north_star quotes
 
 
 def _package():
@@ -162,8 +163,21 @@ def cpu_oracle_rate(n=(256, 256, 256), budget_s: float = 15.0) -> dict:
     o.step(k)
     dt = time.perf_counter() - t
     cells = o.nx * o.ny * o.nz
+    del o
+    # the same sample on one thread, a few steps
+    o1 = oracle.Oracle(scn, 400, threads=1)
+    o1.step(1)
+    t = time.perf_counter()
+    o1.step(2)
+    one = cells * 2 / (time.perf_counter() - t) / 1e9
+    cpu = ""
+    try:
+        cpu = next(l.split(":", 1)[1].strip() for l in open("/proc/cpuinfo") if l.startswith("model name"))
+    except (OSError, StopIteration):
+        pass
     return {"value": cells * k / dt / 1e9, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"scaling box {n[0]}x{n[1]}x{n[2]} ({cells} cells), {k} FP64 steps timed after 5 warm-up steps"}
+            "sample": f"scaling box {n[0]}x{n[1]}x{n[2]} ({cells} cells), {k} FP64 steps timed after 5 warm-up steps",
+            "one_thread_value": one, "cpu_model": cpu}
 
 
 def main():
@@ -307,6 +321,7 @@ def main():
                    "parallelism": f"{world} independent problem(s), one per GPU"},
         "roofline": {"bound": "hbm", "kernel": f"k_step_{dom}", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "frac_of_nominal_8TBs": achieved / NOMINAL_HBM_GBS,
                      "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom],
                      "traffic": traffic},
         "kernel_ms": kern,
@@ -400,6 +415,7 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
             "tiling": tiling, "tuning_ms_per_step": tuning["ms_per_step"],
             "roofline": {"bound": "hbm", "kernel": f"k_batch_half ({dom.upper()})", "achieved": ach, "peak": peak,
                          "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                         "frac_of_nominal_8TBs": ach / NOMINAL_HBM_GBS,
                          "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom]},
             "clocks": clk.summary(), "engine_create_s": create_s}
 
