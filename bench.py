@@ -244,13 +244,19 @@ def main():
     from special_topics_b200.scenario import build_problem_from_scenario
 
     # batched-sweep members are built on host processes started before any GPU work
+    # the sweep's members; with N ranks each takes its share (sharding.partition
+    # on cells x steps, the same on every rank, so nothing is exchanged)
     variants = None
-    if rank == 0 and world == 1 and args.batch_members > 0:
+    if args.batch_members > 0:
         import multiprocessing as mp
         from special_topics_b200 import autotune as _at
+        from special_topics_b200 import sharding
         vsteps = 2 * args.warmup + args.batch_steps + 16 + _at.batch_steps_needed(args.tune_steps)
-        with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-            variants = variant_problems(args.batch_members, max(7000, vsteps), pool)
+        seeds = list(range(args.batch_members))
+        if world > 1:
+            seeds = [seeds[q] for q in sharding.partition(sharding.variant_costs(seeds, 7000), world)[rank]]
+        with mp.get_context("spawn").Pool(max(1, min(16, (os.cpu_count() or 1) // world))) as pool:
+            variants = variant_problems(seeds, max(7000, vsteps), pool)
 
     K, W, P = args.steps, args.warmup, 16
     scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P)
@@ -331,9 +337,24 @@ def main():
         "e2e": e2e,
         "setup_s": setup_s,
     }
-    if variants:
-        line["batched"] = batched_side(variants, K=args.batch_steps, W=args.warmup, tune_steps=args.tune_steps,
-                                       device=local)
+    if variants is not None:
+        if variants:
+            bs = batched_side(variants, K=args.batch_steps, W=args.warmup, tune_steps=args.tune_steps,
+                              device=local, barrier=barrier)
+        else:                       # a rank with no members still takes the same collective steps
+            bs = None
+            barrier()
+            barrier()
+        if world > 1:
+            # whole-sweep rate: all ranks' cells over the slowest rank's time
+            ms = max_over_ranks(bs["ms_per_step"] * args.batch_steps if bs else 0.0)
+            tot = _sum_over_ranks(float(bs["cells"] if bs else 0), dist, local)
+            if bs:
+                bs = dict(bs, value=tot * args.batch_steps / (ms / 1e3) / 1e9, cells=int(tot),
+                          ms_per_step=ms / args.batch_steps, members=args.batch_members,
+                          scaling="strong: the members are split over the ranks")
+        if rank == 0 and bs:
+            line["batched"] = bs
     if rank == 0 and world == 1 and not args.no_fp64:
         line["fp64_plain"] = fp64_side(pkg)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -369,16 +390,24 @@ def _variant_problem(args):
     return build_problem_from_scenario(workloads.ifa_variant(seed, steps=steps), steps, per_cell=False)
 
 
-def variant_problems(count: int, steps: int, pool=None) -> list:
-    """The batched-sweep members (inverted-F variants, seeds 0..count-1)."""
+def variant_problems(seeds, steps: int, pool=None) -> list:
+    """The batched-sweep members (inverted-F variants of the given seeds)."""
     _package()    # results unpickle into the package's classes
-    jobs = [(s, steps) for s in range(count)]
+    jobs = [(int(s), steps) for s in seeds]
     if pool is None:
         return [_variant_problem(j) for j in jobs]
     return pool.map(_variant_problem, jobs)
 
 
-def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, device: int = 0) -> dict:
+def _sum_over_ranks(x: float, dist, local: int) -> float:
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, device: int = 0,
+                 barrier=lambda: None) -> dict:
     """The batched sweep: every member advanced by one set of four launches per
     step (FP32 fields, material tables), launch shape from the batch autotuner."""
     from special_topics_b200 import autotune
@@ -390,8 +419,10 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
         with Batch(engs) as b:
             tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
             b.run(W)
+            barrier()
             with ClockSampler(device) as clk:
                 ms = b.run_timed(K)
+            barrier()
             kern = b.profile_kernels(8)
             cells = b.cells
             tiling = b.tiling()
