@@ -233,6 +233,17 @@ int fdtd_ctx_read_psi(fdtd_ctx* ctx, int faceId, int slot, double* host, long n)
  * cmxzp cmyzp cmxzn cmyzn), laid out [freq][point] like farfield.js:55. */
 int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, long n);
 
+/* Checkpoint / restore (SURVEY's fdtd_save_state / load_state; the reference
+ * has none): the evolving state of a handle -- fields, Psi, port traces,
+ * far-field accumulators, watchdog and step -- to and from a caller buffer
+ * of fdtd_ctx_state_size bytes.  A state loads only into a handle set up
+ * with the same problem (shape, precision, faces, probes, far field);
+ * stepping on from a loaded state gives the results of stepping on from the
+ * saved one. */
+int fdtd_ctx_state_size(fdtd_ctx* ctx, long long* bytes);
+int fdtd_ctx_save_state(fdtd_ctx* ctx, void* buf, long long bytes);
+int fdtd_ctx_load_state(fdtd_ctx* ctx, const void* buf, long long bytes);
+
 /* Far-field accumulator arithmetic of an FP32 problem: 0 = FP64 (default),
  * 1 = Kahan-compensated FP32 pairs (same 8 bytes per value).  Readback
  * returns FP64 either way.  Set before the first step; FP64 problems keep

@@ -190,6 +190,19 @@ class Engine:
             out[name] = (re, im)
         return out
 
+    def save_state(self) -> bytes:
+        """The evolving state (fields, Psi, traces, accumulators, step) as bytes."""
+        n = C.c_longlong()
+        N.check(N.lib().fdtd_ctx_state_size(self._h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        N.check(N.lib().fdtd_ctx_save_state(self._h, buf, n.value))
+        return buf.raw
+
+    def load_state(self, state: bytes) -> None:
+        """Restores a state saved from an engine of the same problem."""
+        buf = C.create_string_buffer(state, len(state))
+        N.check(N.lib().fdtd_ctx_load_state(self._h, buf, len(state)))
+
     def farfield_post(self, theta, phi):
         """Radiated power [nFreq] and directivity D_theta, D_phi [nFreq, nang]
         computed on the device from the accumulators (farfield.js:257-607)."""

@@ -1183,6 +1183,105 @@ int fdtd_ctx_read_farfield(fdtd_ctx* c, int array, double* re, double* im, long 
   return FDTD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Checkpoint / restore of the evolving state: fields, Psi, port traces,
+// far-field accumulators, watchdog and step.  The problem definition
+// (coefficients, tables, sources, probes, boxes) is not part of it: a state
+// loads into a handle set up with the same problem.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct StateHeader {
+  char magic[8];  // "FDTDST1\0"
+  int nx, ny, nz, prec, nsteps, ts, nv, ni, nfreq, kahan;
+  long long psi[6][4];
+  long long ff_values;
+  long long bytes;  // whole state, header included
+};
+
+// The device ranges of a handle's state, in state order.
+std::vector<std::pair<void*, size_t>> state_ranges(fdtd_ctx* c) {
+  std::vector<std::pair<void*, size_t>> r;
+  long long tot = 0;
+  for (int q = 0; q < 6; q++) tot += c->ncomp[q];
+  r.push_back({c->fields, (size_t)tot * c->esz});
+  for (int f = 0; f < 6; f++)
+    for (int s = 0; s < 4; s++)
+      if (c->face[f].present && c->face[f].psi[s]) r.push_back({c->face[f].psi[s], (size_t)c->face[f].n[s] * c->esz});
+  r.push_back({c->V, sizeof(double) * std::max((int)c->vprobe.size(), 1) * (size_t)c->nsteps});
+  r.push_back({c->I, sizeof(double) * std::max((int)c->iprobe.size(), 1) * (size_t)c->nsteps});
+  if (c->nFreq > 0) r.push_back({c->acc, sizeof(double) * (size_t)(c->ffoff[23] + 2LL * c->nFreq * c->ffsz[2])});
+  r.push_back({c->d_status, 2 * sizeof(int)});
+  return r;
+}
+
+StateHeader state_header(fdtd_ctx* c) {
+  StateHeader h{};
+  memcpy(h.magic, "FDTDST1", 8);
+  h.nx = c->nx; h.ny = c->ny; h.nz = c->nz; h.prec = c->prec; h.nsteps = c->nsteps; h.ts = c->ts;
+  h.nv = (int)c->vprobe.size(); h.ni = (int)c->iprobe.size(); h.nfreq = c->nFreq; h.kahan = c->acc_kahan;
+  for (int f = 0; f < 6; f++)
+    for (int s = 0; s < 4; s++) h.psi[f][s] = (c->face[f].present && c->face[f].psi[s]) ? c->face[f].n[s] : 0;
+  h.ff_values = c->nFreq > 0 ? c->ffoff[23] + 2LL * c->nFreq * c->ffsz[2] : 0;
+  long long bytes = sizeof(StateHeader);
+  for (auto& q : state_ranges(c)) bytes += (long long)q.second;
+  h.bytes = bytes;
+  return h;
+}
+
+}  // namespace
+
+int fdtd_ctx_state_size(fdtd_ctx* c, long long* bytes) {
+  if (!c || !bytes) return fail(FDTD_ERR_BADARG, "NULL argument");
+  int rc = ensure_traces(c);
+  if (rc) return rc;
+  *bytes = state_header(c).bytes;
+  return FDTD_OK;
+}
+
+int fdtd_ctx_save_state(fdtd_ctx* c, void* buf, long long bytes) {
+  if (!c || !buf) return fail(FDTD_ERR_BADARG, "NULL argument");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_traces(c);
+  if (rc) return rc;
+  const StateHeader h = state_header(c);
+  if (bytes != h.bytes) return fail(FDTD_ERR_BADARG, "state buffer of %lld bytes, need %lld", bytes, h.bytes);
+  char* p = (char*)buf;
+  memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  for (auto& q : state_ranges(c)) {
+    CK(cudaMemcpyAsync(p, q.first, q.second, cudaMemcpyDeviceToHost, c->stream));
+    p += q.second;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return FDTD_OK;
+}
+
+int fdtd_ctx_load_state(fdtd_ctx* c, const void* buf, long long bytes) {
+  if (!c || !buf) return fail(FDTD_ERR_BADARG, "NULL argument");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_traces(c);
+  if (rc) return rc;
+  StateHeader mine = state_header(c), theirs;
+  if (bytes < (long long)sizeof(StateHeader)) return fail(FDTD_ERR_BADARG, "state buffer too small");
+  memcpy(&theirs, buf, sizeof(theirs));
+  if (memcmp(theirs.magic, "FDTDST1", 8) != 0) return fail(FDTD_ERR_BADARG, "not an engine state");
+  mine.ts = theirs.ts;  // the step is what loading changes
+  if (memcmp(&mine, &theirs, sizeof(StateHeader)) != 0 || bytes != theirs.bytes)
+    return fail(FDTD_ERR_BADARG, "state was saved from a problem of another shape, precision or probe set");
+  if (theirs.ts < 0 || theirs.ts > c->nsteps) return fail(FDTD_ERR_BADARG, "state step %d out of range", theirs.ts);
+  const char* p = (const char*)buf + sizeof(StateHeader);
+  for (auto& q : state_ranges(c)) {
+    CK(cudaMemcpyAsync(q.first, p, q.second, cudaMemcpyHostToDevice, c->stream));
+    p += q.second;
+  }
+  const int dts = theirs.ts - 1;  // the device counter holds the index of the last step run
+  CK(cudaMemcpyAsync(c->d_ts, &dts, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ts = theirs.ts;
+  return FDTD_OK;
+}
+
 int fdtd_ctx_set_dft_accumulator(fdtd_ctx* c, int kahan_fp32) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
   if (kahan_fp32 != 0 && kahan_fp32 != 1) return fail(FDTD_ERR_BADARG, "accumulator mode %d not in {0,1}", kahan_fp32);

@@ -299,3 +299,26 @@ def test_shared_memory_stages_give_identical_table_results(chunk, rows, pf):
     with Engine(build_problem_from_scenario(scn, steps), "f64") as c:
         with pytest.raises(N.FdtdError):
             autotune.set_tiling(c, 8, 4, 3)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32-table"])
+def test_state_checkpoint_resumes_bit_identically(precision):
+    scn, steps = CASES["small-zp"]()
+    p = build_problem_from_scenario(scn, steps, per_cell=(precision == "f64"))
+    with Engine(p, precision) as a, Engine(p, precision) as b:
+        a.run(25)
+        state = a.save_state()
+        a.run(steps - 25)
+        b.load_state(state)
+        assert b.step == 25
+        b.run(steps - 25)
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        assert np.array_equal(a.currents()[0], b.currents()[0])
+        for fld in ("Hx", "Ez"):
+            assert np.array_equal(a.field(fld), b.field(fld))
+        fa, fb = a.farfield(), b.farfield()
+        assert all(np.array_equal(fa[k][0], fb[k][0]) for k in FF_NAMES)
+    other = build_problem_from_scenario(small_scenario(1, "xp"), steps, per_cell=(precision == "f64"))
+    with Engine(other, precision) as c:
+        with pytest.raises(N.FdtdError):
+            c.load_state(state)
