@@ -69,7 +69,13 @@ def compare(ref: dict, other: dict) -> dict:
     at_peak = np.abs(np.take_along_axis(doth - dref, dref.argmax(axis=1)[:, None], axis=1)[:, 0])
     main = dref >= dref.max(axis=1, keepdims=True) - 10.0
     lobe_err = np.array([np.abs(doth[f][main[f]] - dref[f][main[f]]).max() for f in range(dref.shape[0])])
-    return {"s11_max_abs_dB": float(np.abs(other["s11_db"] - ref["s11_db"]).max()),
+    freqs = np.linspace(1e9, 4e9, dref.shape[0])
+    per_f = {"freq_GHz": (freqs / 1e9).round(4).tolist(),
+             "peak_directivity_abs_dB": peak_err.round(4).tolist(),
+             "radp_rel": np.abs(other["radp"] / ref["radp"] - 1).round(5).tolist(),
+             "radp_fp64": ref["radp"].tolist()}
+    return {"per_frequency": per_f,
+            "s11_max_abs_dB": float(np.abs(other["s11_db"] - ref["s11_db"]).max()),
             "zin_max_rel": float(np.abs(zo - zr).max() / np.abs(zr).max()),
             "radp_max_rel": float(np.abs(other["radp"] / ref["radp"] - 1).max()),
             "peak_directivity_max_abs_dB": float(peak_err.max()),
@@ -97,6 +103,9 @@ def main():
     for name, acc in (("f32-table, FP64 accumulators", "f64"), ("f32-table, Kahan FP32 accumulators", "kahan-f32")):
         r32 = run_one(p32, "f32-table", args.steps, acc=acc)
         out[name] = dict(compare(ref, r32), device_ms=r32["device_ms"])
+    # FP32 fields with the reference's per-cell coefficient arrays
+    r32 = run_one(p64, "f32", args.steps)
+    out["f32 per-cell, FP64 accumulators"] = dict(compare(ref, r32), device_ms=r32["device_ms"])
     text = json.dumps(out, indent=1)
     print(text, flush=True)
     if args.out:
