@@ -8,14 +8,15 @@ the part with no counterpart there.
 
 Model of the tail.  After the source pulse has left, the port voltage and
 current of a linear, passive structure ring down as a sum of damped
-sinusoids; for the inverted-F family one mode dominates.  The network maps
-the first `n_in` steps (4x decimated, each channel scaled by its largest
-magnitude) to that mode's frequency and decay rate and to the complex
-amplitudes of V and I at step `n_in`.  The tail of a run stopped at step
-`n_stop` is x(n) = Re(c exp(s (n - n_in) dt)), s = -alpha + j 2 pi f, with
-the amplitudes c refitted by least squares on the steps [n_in, n_stop) that
-were actually run.  The residual energy of that fit is the gate: above the
-threshold the run is not stopped and keeps stepping (plain FDTD).
+sinusoids sum_m Re(c_m exp(s_m t)), s_m = -alpha_m + j 2 pi f_m.  The network
+maps the first `n_in` steps (4x decimated, each channel scaled by its
+largest magnitude) to the run's tail poles s_m (up to K_POLES of them).  At a
+checkpoint the amplitudes c_m are fitted by least squares to the steps
+[n_in, checkpoint) that were actually run, for the network's poles and for
+matrix-pencil poles of those same steps; the best fit's residual energy is
+the gate.  Below the threshold the run stops and its traces are completed
+with the fitted tail; otherwise it keeps stepping (plain FDTD) to the next
+checkpoint.
 
 `EsNet` is the handle of the CUDA network (include/fdtd_b200.h, fdtd_es_*):
 training, gradients and inference all run in the project's own kernels.
@@ -32,7 +33,8 @@ from . import _native as N
 
 ARCH = dict(in_channels=2, in_length=375, conv_layers=4, channels=64, kernel=5, stride=2, mlp_layers=2,
             mlp_width=256)
-OUT_DIM = 6          # f, log alpha, Re/Im c_V, Re/Im c_I
+K_POLES = 6          # tail poles the network predicts
+OUT_DIM = 2 * K_POLES  # per pole: (f - F_CENTER) / F_SCALE and log(alpha / ALPHA_UNIT), sorted by f
 DECIM = 4            # input decimation
 F_CENTER, F_SCALE = 2.5e9, 1.0e9
 ALPHA_UNIT = 1.0e9   # decay rates in 1/ns
@@ -320,84 +322,159 @@ def run_variants(problems, steps: int, precision: str = "f32-table", group: int 
     return V, I, device_s
 
 
+
+
+# ---------------------------------------------------------------------------
+# Pole sets: what the network predicts and what stops a run
+# ---------------------------------------------------------------------------
+PAD_POLE = complex(-5.0e9, 2 * math.pi * 7.5e9)   # fills unused slots: fast decay, above the band
+
+
+def window_poles(V, I, n0: int, n1: int, dt: float, M: int = 12, decim: int = DECIM, fmax: float = 8e9) -> list:
+    """Decaying poles (upper half plane, f <= fmax) of a joint matrix pencil of
+    order M over the decimated V and I samples of [n0, n1)."""
+    sv = float(np.abs(V[n0:n1]).max()) or 1.0
+    si = float(np.abs(I[n0:n1]).max()) or 1.0
+    z = _pencil([np.asarray(V[n0:n1:decim]) / sv, np.asarray(I[n0:n1:decim]) / si], M)
+    out = []
+    for zz in z:
+        if not (zz.imag > 0 or abs(zz.imag) < 1e-12) or zz == 0:
+            continue
+        s_ = complex(np.log(zz)) / (decim * dt)
+        if s_.real < 0 and s_.imag / (2 * math.pi) <= fmax:
+            out.append(s_)
+    return out
+
+
+def poles_to_target(poles, k: int = K_POLES) -> np.ndarray:
+    """Network target of a pole set: the k slowest-decaying poles sorted by
+    frequency, unused slots filled with PAD_POLE."""
+    ps = sorted(poles, key=lambda s_: s_.real, reverse=True)[:k]
+    ps = sorted(ps, key=lambda s_: s_.imag) + [PAD_POLE] * (k - len(ps))
+    y = []
+    for s_ in ps:
+        y += [(s_.imag / (2 * math.pi) - F_CENTER) / F_SCALE, math.log(-s_.real / ALPHA_UNIT)]
+    return np.array(y, np.float32)
+
+
+def target_to_poles(y) -> list:
+    y = np.asarray(y, dtype=np.float64)
+    return [complex(-math.exp(y[2 * q + 1]) * ALPHA_UNIT, 2 * math.pi * (y[2 * q] * F_SCALE + F_CENTER))
+            for q in range(len(y) // 2)]
+
+
+def pole_tail(V, I, poles, n0: int, n_stop: int, n_total: int, dt: float):
+    """Amplitudes of `poles` fitted on the steps [n0, n_stop) that were run;
+    returns the traces over n_total steps (run steps, then the fitted tail)
+    and the larger residual-energy ratio of V and I."""
+    cV, rv = fit_modes(V[n0:n_stop], poles, n0, n0, dt)
+    cI, ri = fit_modes(I[n0:n_stop], poles, n0, n0, dt)
+    t = (np.arange(n_stop, n_total) - n0) * dt
+    tv = np.zeros(t.size)
+    ti = np.zeros(t.size)
+    for c1, c2, s_ in zip(cV, cI, poles):
+        e = np.exp(s_ * t)
+        tv += (c1 * e).real
+        ti += (c2 * e).real
+    return (np.concatenate([np.asarray(V[:n_stop], np.float64), tv]),
+            np.concatenate([np.asarray(I[:n_stop], np.float64), ti]), max(rv, ri))
+
+
 # ---------------------------------------------------------------------------
 # Stopping runs early
 # ---------------------------------------------------------------------------
 @dataclass
 class StopPolicy:
-    """n_in: steps the network reads; n_check: steps run past n_in whose
-    samples refit the amplitudes and measure the residual; max_resid: the
-    residual-energy ratio above which a run is not stopped; n_total: the
-    step count the result stands in for (numberOfTimeSteps)."""
+    """n_in: steps the network reads.  checkpoints: steps at which a run may
+    stop.  At a checkpoint each candidate pole set (the network's, and matrix
+    pencils of the run's own samples since n_in, orders `pencil_orders`) is
+    fitted to [n_in, checkpoint); the best fit stops the run when its
+    residual-energy ratio is at most max_resid, and always at the last
+    checkpoint.  Runs that do not stop keep stepping (plain FDTD) to the next
+    checkpoint.  n_total: the step count the result stands in for."""
     n_in: int = 1500
-    n_check: int = 300
-    max_resid: float = 0.03
+    checkpoints: tuple = (2300, 3000, 4000, 5000)
+    max_resid: float = 1e-4
     n_total: int = 7000
+    pencil_orders: tuple = (8, 12, 16)
     decim: int = DECIM
 
-    @property
-    def n_stop(self) -> int:
-        return self.n_in + self.n_check
+
+def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
+    out = [list(net_poles)] if net_poles else []
+    for M in policy.pencil_orders:
+        try:
+            P = window_poles(V, I, policy.n_in, n1, dt, M, policy.decim)
+        except (ValueError, np.linalg.LinAlgError):
+            continue
+        if P:
+            out.append(P)
+    return out
 
 
-def pencil_mode(V, I, n0: int, n1: int, dt: float, decim: int = DECIM) -> Mode:
-    """The method without the network: the dominant mode estimated from the
-    run's own samples [n0, n1) by the joint matrix pencil."""
-    return dominant_mode(V, I, n0, n1, dt, decim=decim)
-
-
-def decide(V, I, mode: Mode | None, policy: StopPolicy, dt: float):
-    """Refits `mode` on [n_in, n_stop) and applies the residual-energy gate.
-    Returns (accepted, refitted mode or None, residual)."""
-    if mode is None or not (mode.alpha > 0 and math.isfinite(mode.f)):
-        return False, None, float("inf")
-    m, r = refit(V, I, mode, policy.n_stop, dt)
-    return r <= policy.max_resid, m, r
+def best_tail(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None):
+    """(traces over n_total, residual, index of the winning candidate) of the
+    candidate pole set that fits [n_in, n1) best; None when no candidate fits."""
+    best = None
+    for q, P in enumerate(candidate_poles(V, I, n1, dt, policy, net_poles)):
+        try:
+            v, i, r = pole_tail(V, I, P, policy.n_in, n1, policy.n_total, dt)
+        except np.linalg.LinAlgError:
+            continue
+        if np.isfinite(r) and (best is None or r < best[2]):
+            best = (v, i, r, q)
+    return best
 
 
 def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: dict | None = None,
                         use_network: bool = True) -> list[dict]:
-    """Advances FP32 engines of one batch to policy.n_stop, predicts each run's
-    tail mode (the network, or the pencil on the run's own samples when
-    use_network is False), and stops the runs whose refit passes the gate;
-    the others keep stepping to n_total (plain FDTD).  Returns per engine
-    {"V", "I": traces over n_total steps (stopped runs extended with their
-    tail), "stopped_at", "accepted", "resid", "mode"}."""
+    """Advances FP32 engines of one batch through the checkpoints of `policy`
+    and stops each run at the first checkpoint whose best fit passes the gate
+    (the last checkpoint always stops).  With use_network the network's pole
+    set (predicted on the device from the first n_in steps) competes with the
+    pencils.  Returns per engine {"V", "I": traces over n_total steps,
+    "stopped_at", "resid", "winner": "network" or "pencil"}."""
     from .backend import Batch
-    with Batch(engines) as b:
-        if tiling:
-            b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
-        b.run(policy.n_stop - b.step)
-    modes = [None] * len(engines)
-    if use_network:
-        y, scales = net.predict_members(engines, policy.decim)
-        modes = [target_to_mode(y[q], scales[q], policy.n_in) for q in range(len(engines))]
-    out, rest = [], []
-    for q, e in enumerate(engines):
-        dt = e.problem.grid.dt
-        V, I = e.voltages(policy.n_stop)[0], e.currents(policy.n_stop)[0]
-        m = modes[q]
-        if not use_network:
-            try:
-                m = pencil_mode(V, I, policy.n_in, policy.n_stop, dt, policy.decim)
-            except (ValueError, np.linalg.LinAlgError):
-                m = None
-        ok, fit, r = decide(V, I, m, policy, dt)
-        rec = {"accepted": ok, "resid": r, "mode": fit, "stopped_at": policy.n_stop}
-        if ok:
-            rec["V"], rec["I"] = extend(V, I, fit, policy.n_stop, policy.n_total, dt)
-        else:
-            rest.append(q)
-        out.append(rec)
-    if rest:
-        with Batch([engines[q] for q in rest]) as b:
+    out = [None] * len(engines)
+    net_poles = [None] * len(engines)
+    active = list(range(len(engines)))
+    for cp in policy.checkpoints:
+        with Batch([engines[q] for q in active]) as b:
             if tiling:
                 b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
-            b.run(policy.n_total - b.step)
-        for q in rest:
+            b.run(cp - b.step)
+        if use_network and net is not None and net_poles[active[0]] is None:
+            sub = [engines[q] for q in active]
+            for g0 in range(0, len(sub), net.max_batch):
+                y, _ = net.predict_members(sub[g0:g0 + net.max_batch], policy.decim)
+                for k, q in enumerate(active[g0:g0 + net.max_batch]):
+                    net_poles[q] = target_to_poles(y[k])
+        rest = []
+        for q in active:
             e = engines[q]
-            out[q]["V"], out[q]["I"] = e.voltages(policy.n_total)[0], e.currents(policy.n_total)[0]
-            out[q]["stopped_at"] = policy.n_total
+            dt = e.problem.grid.dt
+            V, I = e.voltages(cp)[0], e.currents(cp)[0]
+            got = best_tail(V, I, cp, dt, policy, net_poles[q] if use_network else None)
+            last = cp == policy.checkpoints[-1]
+            if got is not None and (got[2] <= policy.max_resid or last):
+                v, i, r, w = got
+                out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
+                          "winner": "network" if (use_network and net_poles[q] and w == 0) else "pencil"}
+            else:                          # keeps stepping (at the last checkpoint: to n_total)
+                rest.append(q)
+        if cp == policy.checkpoints[-1]:
+            break
+        active = rest
+        if not active:
+            break
+    leftover = [q for q in range(len(engines)) if out[q] is None]
+    if leftover:
+        with Batch([engines[q] for q in leftover]) as b:
+            b.run(policy.n_total - b.step)
+        for q in leftover:
+            e = engines[q]
+            out[q] = {"V": e.voltages(policy.n_total)[0], "I": e.currents(policy.n_total)[0],
+                      "stopped_at": policy.n_total, "resid": float("nan"), "winner": "full run"}
     return out
 
 

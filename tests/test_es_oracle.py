@@ -90,3 +90,30 @@ def test_refit_residual_separates_one_mode_from_two():
     Ve, _ = ES.extend(V, I, got, 1800, 7000, dt)
     full_V, _ = _ringing(m, 7000)
     assert len(Ve) == 7000 and np.allclose(Ve, full_V, atol=1e-12)
+
+
+def test_pole_targets_round_trip_and_pad():
+    poles = [complex(-0.4e9, 2 * np.pi * 2.1e9), complex(-2.0e9, 2 * np.pi * 6.6e9), complex(-0.2e9, 2 * np.pi * 0.7e9)]
+    y = ES.poles_to_target(poles)
+    assert y.shape == (ES.OUT_DIM,)
+    back = ES.target_to_poles(y)
+    got = sorted(back[:3], key=lambda s: s.imag)
+    want = sorted(poles, key=lambda s: s.imag)
+    for a, b in zip(got, want):
+        assert abs(a - b) / abs(b) < 1e-6
+    assert all(abs(p - ES.PAD_POLE) / abs(ES.PAD_POLE) < 1e-6 for p in back[3:])
+
+
+def test_window_poles_and_tail_recover_two_modes():
+    dt = 8.666e-13
+    m1 = ES.Mode(2.09e9, 0.45e9, 0.011 - 0.004j, 1.5e-4 + 2e-5j, 1500)
+    m2 = ES.Mode(2.61e9, 0.9e9, 0.004 + 0.002j, -4e-5 + 1e-5j, 1500)
+    V, I = _ringing(m1, 7000, extra=m2)
+    P = ES.window_poles(V, I, 1500, 3500, dt, M=4)
+    assert len(P) == 2
+    v, i, r = ES.pole_tail(V, I, P, 1500, 2300, 7000, dt)
+    assert r < 1e-12
+    assert np.allclose(v, V, atol=1e-9) and np.allclose(i, I, atol=1e-11)
+    pol = ES.StopPolicy(pencil_orders=(4,))
+    got = ES.best_tail(V, I, 2300, dt, pol)
+    assert got is not None and got[2] < 1e-12
