@@ -187,6 +187,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", default="512x512x640")
+    ap.add_argument("--ncpml", type=int, default=8, help="CPML cells per face of the scaling box (0: PEC walls)")
     ap.add_argument("--precision", default="f32-table", choices=["f32-table", "f32", "f64"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 side measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
@@ -259,7 +260,7 @@ def main():
             variants = variant_problems(seeds, max(7000, vsteps), pool)
 
     K, W, P = args.steps, args.warmup, 16
-    scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P)
+    scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P, ncpml=args.ncpml)
     t0 = time.perf_counter()
     prob = build_problem_from_scenario(scn, K + W + P, per_cell=(args.precision != "f32-table"))
     setup_s = time.perf_counter() - t0
@@ -272,7 +273,7 @@ def main():
         ch, rw, pf = (int(x) for x in args.tiling.split(","))
         tuning = {"chunk": ch, "rows": rw, "prefetch": pf, "ms_per_step": None}
     elif not args.no_tune:
-        scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000), 3000,
+        scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000, ncpml=args.ncpml), 3000,
                                               per_cell=(args.precision != "f32-table"))
         tuning = autotune.tune(scratch, args.precision, device=local, steps_per_candidate=args.tune_steps)
         del scratch

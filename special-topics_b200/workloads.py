@@ -26,9 +26,10 @@ MM = 1e-3
 
 
 def _boundary(ncpml: int, air: int) -> dict:
+    """CPML of `ncpml` cells on every face; ncpml = 0 gives PEC walls."""
     b = {}
     for f in ("xn", "xp", "yn", "yp", "zn", "zp"):
-        b[f"type_{f}"] = "cpml"
+        b[f"type_{f}"] = "cpml" if ncpml > 0 else "pec"
         b[f"air_buffer_{f}"] = air
         b[f"cpml_cells_{f}"] = ncpml
     b.update({"cpml_order": 3, "cpml_sigma_factor": 1.3, "cpml_kappa_max": 7,
