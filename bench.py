@@ -197,6 +197,7 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
+    ap.add_argument("--batch-tiling", default=None, help="fixed batch shape chunk,rows,prefetch,group (skips the tuner)")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
@@ -341,7 +342,7 @@ def main():
     if variants is not None:
         if variants:
             bs = batched_side(variants, K=args.batch_steps, W=args.warmup, tune_steps=args.tune_steps,
-                              device=local, barrier=barrier)
+                              device=local, barrier=barrier, fixed=args.batch_tiling)
         else:                       # a rank with no members still takes the same collective steps
             bs = None
             barrier()
@@ -408,7 +409,7 @@ def _sum_over_ranks(x: float, dist, local: int) -> float:
 
 
 def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, device: int = 0,
-                 barrier=lambda: None) -> dict:
+                 barrier=lambda: None, fixed: str | None = None) -> dict:
     """The batched sweep: every member advanced by one set of four launches per
     step (FP32 fields, material tables), launch shape from the batch autotuner."""
     from special_topics_b200 import autotune
@@ -418,7 +419,12 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
     create_s = time.perf_counter() - t0
     try:
         with Batch(engs) as b:
-            tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
+            if fixed:
+                ch, rw, pf, gp = (int(x) for x in fixed.split(","))
+                b.set_tiling(ch, rw, pf, gp)
+                tuning = {"ms_per_step": None}
+            else:
+                tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
             b.run(W)
             barrier()
             with ClockSampler(device) as clk:
