@@ -25,6 +25,8 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -190,16 +192,25 @@ class Mode:
         return (c * np.exp(self.s() * t)).real
 
 
-def _pencil(signals, M: int) -> np.ndarray:
-    """Matrix-pencil poles (per sample) shared by several equally sampled signals."""
+def _pencil_orders(signals, orders) -> list:
+    """Matrix-pencil poles (per sample) shared by several equally sampled
+    signals, for each model order in `orders` (one SVD serves all)."""
     Ys = []
     for x in signals:
         L = len(x) // 3
         Ys.append(np.lib.stride_tricks.sliding_window_view(np.asarray(x, dtype=np.float64), L + 1))
     Y = np.concatenate(Ys, axis=0)
     _, _, Vh = np.linalg.svd(Y, full_matrices=False)
-    Vm = Vh[:M].conj().T
-    return np.linalg.eigvals(np.linalg.pinv(Vm[:-1]) @ Vm[1:])
+    out = []
+    for M in orders:
+        Vm = Vh[:M].conj().T
+        out.append(np.linalg.eigvals(np.linalg.pinv(Vm[:-1]) @ Vm[1:]))
+    return out
+
+
+def _pencil(signals, M: int) -> np.ndarray:
+    """Matrix-pencil poles (per sample) shared by several equally sampled signals."""
+    return _pencil_orders(signals, (M,))[0]
 
 
 def fit_modes(x, poles, n0: int, n_start: int, dt: float):
@@ -330,20 +341,28 @@ def run_variants(problems, steps: int, precision: str = "f32-table", group: int 
 PAD_POLE = complex(-5.0e9, 2 * math.pi * 7.5e9)   # fills unused slots: fast decay, above the band
 
 
-def window_poles(V, I, n0: int, n1: int, dt: float, M: int = 12, decim: int = DECIM, fmax: float = 8e9) -> list:
-    """Decaying poles (upper half plane, f <= fmax) of a joint matrix pencil of
-    order M over the decimated V and I samples of [n0, n1)."""
+def window_poles_orders(V, I, n0: int, n1: int, dt: float, orders=(12,), decim: int = DECIM,
+                        fmax: float = 8e9) -> list:
+    """Decaying poles (upper half plane, f <= fmax) of joint matrix pencils of
+    the given orders over the decimated V and I samples of [n0, n1)."""
     sv = float(np.abs(V[n0:n1]).max()) or 1.0
     si = float(np.abs(I[n0:n1]).max()) or 1.0
-    z = _pencil([np.asarray(V[n0:n1:decim]) / sv, np.asarray(I[n0:n1:decim]) / si], M)
-    out = []
-    for zz in z:
-        if not (zz.imag > 0 or abs(zz.imag) < 1e-12) or zz == 0:
-            continue
-        s_ = complex(np.log(zz)) / (decim * dt)
-        if s_.real < 0 and s_.imag / (2 * math.pi) <= fmax:
-            out.append(s_)
-    return out
+    sets = []
+    for z in _pencil_orders([np.asarray(V[n0:n1:decim]) / sv, np.asarray(I[n0:n1:decim]) / si], orders):
+        out = []
+        for zz in z:
+            if not (zz.imag > 0 or abs(zz.imag) < 1e-12) or zz == 0:
+                continue
+            s_ = complex(np.log(zz)) / (decim * dt)
+            if s_.real < 0 and s_.imag / (2 * math.pi) <= fmax:
+                out.append(s_)
+        sets.append(out)
+    return sets
+
+
+def window_poles(V, I, n0: int, n1: int, dt: float, M: int = 12, decim: int = DECIM, fmax: float = 8e9) -> list:
+    """window_poles_orders for one order."""
+    return window_poles_orders(V, I, n0, n1, dt, (M,), decim, fmax)[0]
 
 
 def poles_to_target(poles, k: int = K_POLES) -> np.ndarray:
@@ -402,14 +421,11 @@ class StopPolicy:
 
 def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
     out = [list(net_poles)] if net_poles else []
-    for M in policy.pencil_orders:
-        try:
-            P = window_poles(V, I, policy.n_in, n1, dt, M, policy.decim)
-        except (ValueError, np.linalg.LinAlgError):
-            continue
-        if P:
-            out.append(P)
-    return out
+    try:
+        sets = window_poles_orders(V, I, policy.n_in, n1, dt, policy.pencil_orders, policy.decim)
+    except (ValueError, np.linalg.LinAlgError):
+        sets = []
+    return out + [P for P in sets if P]
 
 
 def best_tail(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None):
@@ -450,12 +466,19 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                 for k, q in enumerate(active[g0:g0 + net.max_batch]):
                     net_poles[q] = target_to_poles(y[k])
         rest = []
-        for q in active:
-            e = engines[q]
-            dt = e.problem.grid.dt
-            V, I = e.voltages(cp)[0], e.currents(cp)[0]
-            got = best_tail(V, I, cp, dt, policy, net_poles[q] if use_network else None)
-            last = cp == policy.checkpoints[-1]
+        last = cp == policy.checkpoints[-1]
+        traces = [(engines[q].voltages(cp)[0], engines[q].currents(cp)[0]) for q in active]
+
+        def fit_one(k):
+            q = active[k]
+            return best_tail(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
+                             net_poles[q] if use_network else None)
+
+        # the fits are LAPACK-bound and release the GIL: one thread per host core
+        with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+            fits = list(ex.map(fit_one, range(len(active))))
+        for k, q in enumerate(active):
+            got = fits[k]
             if got is not None and (got[2] <= policy.max_resid or last):
                 v, i, r, w = got
                 out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
