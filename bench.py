@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
     ap.add_argument("--batch-tiling", default=None, help="fixed batch shape chunk,rows,prefetch,group (skips the tuner)")
+    ap.add_argument("--ttS11-members", dest="ttS11_members", type=int, default=64,
+                    help="held-out variants of the time-to-S11 leg (0: skip)")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
@@ -357,6 +359,11 @@ def main():
                           scaling="strong: the members are split over the ranks")
         if rank == 0 and bs:
             line["batched"] = bs
+    if rank == 0 and world == 1 and args.ttS11_members > 0:
+        try:
+            line["time_to_s11"] = time_to_s11_side(args.ttS11_members, device=local)
+        except Exception as e:  # this leg must not hide the main number
+            line["time_to_s11"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_fp64:
         line["fp64_plain"] = fp64_side(pkg)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -456,6 +463,68 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
                          "frac_of_nominal_8TBs": ach / NOMINAL_HBM_GBS,
                          "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom]},
             "clocks": clk.summary(), "engine_create_s": create_s}
+
+
+WEIGHTS = os.path.join(ROOT, "special-topics_b200", "weights", "es_ifa_variants.npz")
+
+
+def time_to_s11_side(count: int, device: int = 0) -> dict:
+    """Time-to-S11 on held-out inverted-F variants (seeds 10000..): plain FP64
+    batched runs of all 7000 steps against FP32 runs stopped by the checkpoint
+    rule, with the trained network's poles competing and without them.  Each
+    time runs from the first step launch to S11 on the host (301 points,
+    1-4 GHz), the stop rule's fits and inference included, engine set-up
+    excluded."""
+    import multiprocessing as mp
+    from special_topics_b200 import earlystop as ES
+    from special_topics_b200.backend import Batch, Engine
+    if not os.path.exists(WEIGHTS):
+        return {"unavailable": "no trained weights in special-topics_b200/weights"}
+    seeds = list(range(10000, 10000 + count))
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        probs = variant_problems(seeds, 7000, pool)
+        probs64 = pool.map(_variant_problem_f64, [(s_, 7000) for s_ in seeds])
+    freqs = ES.S11_FREQS
+    policy = ES.StopPolicy()
+    tiling = {"chunk": 32, "rows": 4, "prefetch": 1, "group": 0}
+    net = ES.EsNet.load(WEIGHTS, max_batch=max(count, 1), device=device)
+    out = {"workload": f"ifa-variants-{count} (seeds {seeds[0]}..{seeds[-1]})", "steps": policy.n_total}
+    engs = [Engine(p, "f64", device=device) for p in probs64]
+    try:
+        t0 = time.perf_counter()
+        with Batch(engs) as b:
+            b.run(policy.n_total)
+        ref = [ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs) for e in engs]
+        out["plain_f64_s"] = time.perf_counter() - t0
+    finally:
+        for e in engs:
+            e.close()
+    for name, use in (("learned", True), ("no_network", False)):
+        engs = [Engine(p, "f32-table", device=device) for p in probs]
+        try:
+            t0 = time.perf_counter()
+            res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use)
+            s11 = [ES.s11_db(r["V"], r["I"], e.problem.grid.dt, freqs) for r, e in zip(res, engs)]
+            t = time.perf_counter() - t0
+        finally:
+            for e in engs:
+                e.close()
+        err = np.array([np.abs(a - b).max() for a, b in zip(s11, ref)])
+        out[name] = {"time_s": t, "within_0p1_dB": float(np.mean(err <= 0.1)),
+                     "mean_stop_step": float(np.mean([r["stopped_at"] for r in res])),
+                     "max_err_dB_median": float(np.median(err))}
+    net.close()
+    out["ratio_plain_f64_over_learned"] = out["plain_f64_s"] / out["learned"]["time_s"]
+    out["ratio_plain_f64_over_no_network"] = out["plain_f64_s"] / out["no_network"]["time_s"]
+    return out
+
+
+def _variant_problem_f64(args):
+    seed, steps = args
+    _package()
+    from special_topics_b200 import workloads
+    from special_topics_b200.scenario import build_problem_from_scenario
+    return build_problem_from_scenario(workloads.ifa_variant(seed, steps=steps), steps)
 
 
 def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
