@@ -386,14 +386,26 @@ struct HBand {
   T ca[3], cb[3];       // their CPsi (per-cell layouts; unused with tables)
 };
 
-template <typename T, class C>
+// Face mask F of a band plane: bit 0 = an x band may hold the plane (uniform
+// over the warp), bit 1 = the warp's row lies in a y band, bit 2 = some lane
+// of the warp lies in a z band.  Faces outside the mask are compiled out;
+// faces inside it are still tested per lane.
+constexpr unsigned kFX = 1, kFY = 2, kFZ = 4, kFAll = 7;
+
+template <typename T, class C, unsigned F = kFAll>
 __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
                                             HBand<T, C>& in) {
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
   const Fields<T>& f = p.f;
-  in.xf = band_face(p.face, 0, i, false, in.xci);
-  in.kmx = p.coef.invk(3, i);
+  if (F & kFX) {
+    in.xf = band_face(p.face, 0, i, false, in.xci);
+    in.kmx = p.coef.invk(3, i);
+  } else {
+    in.xf = -1;
+    in.xci = 0;
+    in.kmx = 1.f;
+  }
   in.v.ez_n = T(0);
   in.v.ey_n = T(0);
   if (c.hx_ok) {
@@ -402,13 +414,13 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
     in.v.ey_kp = f.Ey[i * sHzEy + c.ob + 1];
     in.v.ez_jp = f.Ez[i * sHyEz + c.oa + nz];
     in.v.r0 = p.coef.fetch(0, idx);
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       const int pi = (i * F.nc + cb.yci) * nz + c.k;
       in.pa[0] = F.psi[0][pi];
       in.ca[0] = p.coef.cpsi_fetch(F, 0, pi);
     }
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       const int pi = (i * ny + c.j) * F.nc + cb.zci;
       in.pb[0] = F.psi[0][pi];
@@ -430,7 +442,7 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
         in.pa[1] = F.psi[0][pi];
         in.ca[1] = p.coef.cpsi_fetch(F, 0, pi);
       }
-      if (cb.zf >= 0) {
+      if ((F & kFZ) && cb.zf >= 0) {
         const Face<T>& F = p.face[cb.zf];
         const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
         in.pb[1] = F.psi[1][pi];
@@ -449,7 +461,7 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
         in.pa[2] = F.psi[1][pi];
         in.ca[2] = p.coef.cpsi_fetch(F, 1, pi);
       }
-      if (cb.yf >= 0) {
+      if ((F & kFY) && cb.yf >= 0) {
         const Face<T>& F = p.face[cb.yf];
         const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
         in.pb[2] = F.psi[1][pi];
@@ -461,9 +473,10 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
 
 // h_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
 // arithmetic in the identical order.
-template <typename T, class C, bool EXACT>
+template <typename T, class C, bool EXACT, unsigned F = kFAll>
 __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
                                              const HBand<T, C>& in, T& ez_c, T& ey_c) {
+  const float kmy = (F & kFY) ? c.kmy : 1.f, kmz = (F & kFZ) ? c.kmz : 1.f;
   using A = Ar<T, EXACT>;
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1;
@@ -473,14 +486,14 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
   if (c.hx_ok) {
     const T dey = A::dif(in.v.ey_kp, ey_c);
     const T dez = A::dif(in.v.ez_jp, ez_c);
-    p.coef.decode_k(0, in.v.r0, c.kmz, c.kmy, c0, c1, c2, u1, u2);
+    p.coef.decode_k(0, in.v.r0, kmz, kmy, c0, c1, c2, u1, u2);
     T h = A::lin3(c0, in.v.hx, c1, dey, c2, dez);
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 0, in.pa[0], in.ca[0],
                                             dez, u2, dy, h);
     }
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 0, in.pb[0], in.cb[0],
                                             dey, u1, dz, h);
@@ -491,12 +504,12 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
     if (c.hy_ok) {
       const T dez = A::dif(in.v.ez_n, ez_c);
       const T dex = A::dif(in.v.ex_kp, in.v.ex);
-      p.coef.decode_k(1, in.v.r1, in.kmx, c.kmz, c0, c1, c2, u1, u2);
+      p.coef.decode_k(1, in.v.r1, in.kmx, kmz, c0, c1, c2, u1, u2);
       T h = A::lin3(c0, in.v.hy, c1, dez, c2, dex);
-      if (in.xf >= 0)
+      if ((F & kFX) && in.xf >= 0)
         cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 0, in.pa[1],
                                               in.ca[1], dez, u1, dx, h);
-      if (cb.zf >= 0) {
+      if ((F & kFZ) && cb.zf >= 0) {
         const Face<T>& F = p.face[cb.zf];
         cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 1, in.pb[1],
                                               in.cb[1], dex, u2, dz, h);
@@ -506,12 +519,12 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
     if (c.hz_ok) {
       const T dex = A::dif(in.v.ex_jp, in.v.ex);
       const T dey = A::dif(in.v.ey_n, ey_c);
-      p.coef.decode_k(2, in.v.r2, c.kmy, in.kmx, c0, c1, c2, u1, u2);
+      p.coef.decode_k(2, in.v.r2, kmy, in.kmx, c0, c1, c2, u1, u2);
       T h = A::lin3(c0, in.v.hz, c1, dex, c2, dey);
-      if (in.xf >= 0)
+      if ((F & kFX) && in.xf >= 0)
         cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 1, in.pa[2],
                                               in.ca[2], dey, u2, dx, h);
-      if (cb.yf >= 0) {
+      if ((F & kFY) && cb.yf >= 0) {
         const Face<T>& F = p.face[cb.yf];
         cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 1, in.pb[2],
                                               in.cb[2], dex, u1, dy, h);
@@ -525,22 +538,22 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
 
 // Planes [a, b) of a column in the band form: every load of a plane is
 // issued before its stores; with BPF the next plane's loads are also in flight.
-template <typename T, class C, bool EXACT, bool BPF>
+template <typename T, class C, bool EXACT, bool BPF, unsigned F = kFAll>
 __device__ __forceinline__ void h_band_range(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int a,
                                              int b, T& ez_c, T& ey_c) {
   if (a >= b) return;
   HBand<T, C> cur, nxt;
   if (!BPF) {
     for (int i = a; i < b; i++) {
-      h_band_load(p, c, cb, i, cur);
-      h_band_store<T, C, EXACT>(p, c, cb, i, cur, ez_c, ey_c);
+      h_band_load<T, C, F>(p, c, cb, i, cur);
+      h_band_store<T, C, EXACT, F>(p, c, cb, i, cur, ez_c, ey_c);
     }
     return;
   }
-  h_band_load(p, c, cb, a, cur);
+  h_band_load<T, C, F>(p, c, cb, a, cur);
   for (int i = a; i < b; i++) {
-    if (i + 1 < b) h_band_load(p, c, cb, i + 1, nxt);
-    h_band_store<T, C, EXACT>(p, c, cb, i, cur, ez_c, ey_c);
+    if (i + 1 < b) h_band_load<T, C, F>(p, c, cb, i + 1, nxt);
+    h_band_store<T, C, EXACT, F>(p, c, cb, i, cur, ez_c, ey_c);
     cur = nxt;
   }
 }
@@ -671,56 +684,11 @@ struct MinBlocks {
   static constexpr int value = sizeof(T) == 8 ? 2 : (PF == 2 ? 3 : 4);
 };
 
-// H update of one tile: columns (bx*32 + tx, by*rows + ty), x planes from
-// bz*ichunk.  PF: how many planes ahead the interior loop loads (1 or 2).
+// Lean planes [xa, xb) of an H column: register prefetch (PF 1, 2) or
+// shared-memory stages (PF 3, 4, material tables).
 template <typename T, class C, bool EXACT, int PF>
-__device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
-  const int k = bx * blockDim.x + threadIdx.x;
-  const int j = by * blockDim.y + threadIdx.y;
-  const int i0 = bz * p.ichunk;
-  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
-  const bool valid = j <= ny && k <= nz;
-  HCol<T> c;
-  c.j = j;
-  c.k = k;
-  c.oa = j * nz + k;
-  c.ob = j * (nz + 1) + k;
-  c.hx_ok = j < ny && k < nz;
-  c.hy_ok = k < nz;
-  c.hz_ok = j < ny;
-  c.yn = band_ci(p.face[2], j, false);
-  c.yp = band_ci(p.face[3], j, false);
-  c.zn = band_ci(p.face[4], k, false);
-  c.zp = band_ci(p.face[5], k, false);
-  // a warp is 32 consecutive k of one j: it takes the lean path when none of
-  // its columns lies in a y or z band
-  const bool lean_col = !valid || (c.yn < 0 && c.yp < 0 && c.zn < 0 && c.zp < 0);
-  const bool warp_lean = __all_sync(0xffffffffu, lean_col);
-  if (!valid) return;
-  c.kmy = p.coef.invk(4, j);
-  c.kmz = p.coef.invk(5, k);
-  const int i1 = min(i0 + p.ichunk, nx + 1);
-  // carried x-neighbours: Ez(i,j,k), Ey(i,j,k)
-  T ez_c = c.hy_ok ? p.f.Ez[i0 * (ny + 1) * nz + c.oa] : T(0);
-  T ey_c = c.hz_ok ? p.f.Ey[i0 * ny * (nz + 1) + c.ob] : T(0);
-  // interior planes [xa, xb): outside both x bands and below nx
-  int xa = i1, xb = i1;
-  if (warp_lean) {
-    const int lo = p.face[0].nc > 0 ? p.face[0].m_start + p.face[0].nc : 0;
-    const int hi = p.face[1].nc > 0 ? p.face[1].m_start : nx;
-    xa = min(max(i0, lo), i1);
-    xb = max(xa, min(i1, hi));
-  }
-  ColBands cb{};
-  constexpr bool BPF = BandForm<C>::kPrefetch;
-  const bool band_form = BandForm<C>::kUse && p.bands_disjoint != 0;
-  if (band_form) {
-    cb.yf = band_face(p.face, 1, j, false, cb.yci);
-    cb.zf = band_face(p.face, 2, k, false, cb.zci);
-    h_band_range<T, C, EXACT, BPF>(p, c, cb, i0, xa, ez_c, ey_c);
-  } else {
-    for (int i = i0; i < xa; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
-  }
+__device__ __forceinline__ void h_lean_range(const StepParams<T, C>& p, const HCol<T>& c, int xa, int xb, T& ez_c,
+                                             T& ey_c) {
   if constexpr (PF >= 3 && C::kTable) {
     h_staged_range<PF>(p, c, xa, xb, ez_c, ey_c);
   } else if (xa < xb) {
@@ -740,10 +708,84 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
       if (PF == 2) nxt = nx2;
     }
   }
-  if (band_form)
-    h_band_range<T, C, EXACT, BPF>(p, c, cb, xb, i1, ez_c, ey_c);
+}
+
+// Planes [i0, i1) of an H column in the band form, for a warp whose y/z
+// band membership is YZ: the edge planes (an x band may apply) with x added,
+// the x-interior planes [xa, xb) with YZ only, or lean when YZ is empty.
+template <typename T, class C, bool EXACT, int PF, unsigned YZ>
+__device__ __forceinline__ void h_tile_planes(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i0,
+                                              int xa, int xb, int i1, T& ez_c, T& ey_c) {
+  constexpr bool BPF = BandForm<C>::kPrefetch;
+  h_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, i0, xa, ez_c, ey_c);
+  if constexpr (YZ == 0)
+    h_lean_range<T, C, EXACT, PF>(p, c, xa, xb, ez_c, ey_c);
   else
-    for (int i = xb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+    h_band_range<T, C, EXACT, BPF, YZ>(p, c, cb, xa, xb, ez_c, ey_c);
+  h_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, xb, i1, ez_c, ey_c);
+}
+
+// H update of one tile: columns (bx*32 + tx, by*rows + ty), x planes from
+// bz*ichunk.  PF: how many planes ahead the interior loop loads.
+template <typename T, class C, bool EXACT, int PF>
+__device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
+  const int k = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int i0 = bz * p.ichunk;
+  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
+  const bool valid = j <= ny && k <= nz;
+  HCol<T> c;
+  c.j = j;
+  c.k = k;
+  c.oa = j * nz + k;
+  c.ob = j * (nz + 1) + k;
+  c.hx_ok = j < ny && k < nz;
+  c.hy_ok = k < nz;
+  c.hz_ok = j < ny;
+  c.yn = band_ci(p.face[2], j, false);
+  c.yp = band_ci(p.face[3], j, false);
+  c.zn = band_ci(p.face[4], k, false);
+  c.zp = band_ci(p.face[5], k, false);
+  // a warp is 32 consecutive k of one j: y band membership is uniform over
+  // it, z band membership is per lane
+  const bool ycol = c.yn >= 0 || c.yp >= 0, zcol = c.zn >= 0 || c.zp >= 0;
+  const bool warp_lean = __all_sync(0xffffffffu, !valid || (!ycol && !zcol));
+  const bool warp_y = __any_sync(0xffffffffu, valid && ycol);
+  const bool warp_z = __any_sync(0xffffffffu, valid && zcol);
+  if (!valid) return;
+  c.kmy = p.coef.invk(4, j);
+  c.kmz = p.coef.invk(5, k);
+  const int i1 = min(i0 + p.ichunk, nx + 1);
+  // carried x-neighbours: Ez(i,j,k), Ey(i,j,k)
+  T ez_c = c.hy_ok ? p.f.Ez[i0 * (ny + 1) * nz + c.oa] : T(0);
+  T ey_c = c.hz_ok ? p.f.Ey[i0 * ny * (nz + 1) + c.ob] : T(0);
+  // x-interior planes [xa, xb): outside both x bands and below nx
+  const int lo = p.face[0].nc > 0 ? p.face[0].m_start + p.face[0].nc : 0;
+  const int hi = p.face[1].nc > 0 ? p.face[1].m_start : nx;
+  const int xa = min(max(i0, lo), i1);
+  const int xb = max(xa, min(i1, hi));
+  if (BandForm<C>::kUse && p.bands_disjoint != 0) {
+    ColBands cb{};
+    cb.yf = band_face(p.face, 1, j, false, cb.yci);
+    cb.zf = band_face(p.face, 2, k, false, cb.zci);
+    if (warp_y) {
+      if (warp_z)
+        h_tile_planes<T, C, EXACT, PF, kFY | kFZ>(p, c, cb, i0, xa, xb, i1, ez_c, ey_c);
+      else
+        h_tile_planes<T, C, EXACT, PF, kFY>(p, c, cb, i0, xa, xb, i1, ez_c, ey_c);
+    } else {
+      if (warp_z)
+        h_tile_planes<T, C, EXACT, PF, kFZ>(p, c, cb, i0, xa, xb, i1, ez_c, ey_c);
+      else
+        h_tile_planes<T, C, EXACT, PF, 0>(p, c, cb, i0, xa, xb, i1, ez_c, ey_c);
+    }
+    return;
+  }
+  // plane-at-a-time form for the band planes; lean interior for lean warps
+  const int la = warp_lean ? xa : i1, lb = warp_lean ? xb : i1;
+  for (int i = i0; i < la; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
+  h_lean_range<T, C, EXACT, PF>(p, c, la, lb, ez_c, ey_c);
+  for (int i = lb; i < i1; i++) h_plane<T, C, EXACT, false>(p, c, i, ez_c, ey_c);
 }
 
 template <typename T, class C, bool EXACT, int PF>
@@ -1003,7 +1045,7 @@ struct EBand {
   T ca[3], cb[3];
 };
 
-template <typename T, class C>
+template <typename T, class C, unsigned F = kFAll>
 __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
                                             EBand<T, C>& in) {
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
@@ -1012,8 +1054,14 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
   const bool inx = i < nx;
   in.hz_i = c.ey_ok ? (inx ? f.Hz[i * sHzEy + c.ob] : p.ex0b[c.ob]) : T(0);
   in.hy_i = c.ez_ok ? (inx ? f.Hy[i * sHyEz + c.oa] : f.Hz[c.oa]) : T(0);
-  in.xf = band_face(p.face, 0, i, true, in.xci);
-  in.kex = p.coef.invk(0, i);
+  if (F & kFX) {
+    in.xf = band_face(p.face, 0, i, true, in.xci);
+    in.kex = p.coef.invk(0, i);
+  } else {
+    in.xf = -1;
+    in.xci = 0;
+    in.kex = 1.f;
+  }
   in.hx_c = (c.ey_ok && c.ez_ok) ? f.Hx[i * sHx + c.oa] : T(0);
   if (inx) {
     const int idx = i * sEx + c.ob;
@@ -1021,13 +1069,13 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     if (c.jy) in.hz_jm = f.Hz[i * sHzEy + c.ob - nzp1];
     if (c.kz) in.hy_km = f.Hy[i * sHyEz + c.oa - 1];
     in.r0 = p.coef.fetch(3, idx);
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
       in.pa[0] = F.psi[3][pi];
       in.ca[0] = p.coef.cpsi_fetch(F, 3, pi);
     }
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
       in.pb[0] = F.psi[2][pi];
@@ -1039,13 +1087,13 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     in.ey = f.Ey[idx];
     if (c.kz) in.hx_km = f.Hx[i * sHx + c.oa - 1];
     in.r1 = p.coef.fetch(4, idx);
-    if (in.xf >= 0) {
+    if ((F & kFX) && in.xf >= 0) {
       const Face<T>& F = p.face[in.xf];
       const int pi = in.xci * sHzEy + c.ob;
       in.pa[1] = F.psi[2][pi];
       in.ca[1] = p.coef.cpsi_fetch(F, 2, pi);
     }
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       const int pi = (i * ny + c.j) * F.nc + cb.zci;
       in.pb[1] = F.psi[3][pi];
@@ -1057,13 +1105,13 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     in.ez = f.Ez[idx];
     if (c.jy) in.hx_jm = f.Hx[i * sHx + c.oa - nz];
     in.r2 = p.coef.fetch(5, idx);
-    if (in.xf >= 0) {
+    if ((F & kFX) && in.xf >= 0) {
       const Face<T>& F = p.face[in.xf];
       const int pi = in.xci * sHyEz + c.oa;
       in.pa[2] = F.psi[3][pi];
       in.ca[2] = p.coef.cpsi_fetch(F, 3, pi);
     }
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       const int pi = (i * F.nc + cb.yci) * nz + c.k;
       in.pb[2] = F.psi[2][pi];
@@ -1074,9 +1122,10 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
 
 // e_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
 // arithmetic in the identical order.
-template <typename T, class C, bool EXACT>
+template <typename T, class C, bool EXACT, unsigned F = kFAll>
 __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
                                              int ts, const EBand<T, C>& in, T& hz_p, T& hy_p) {
+  const float key = (F & kFY) ? c.key : 1.f, kez = (F & kFZ) ? c.kez : 1.f;
   using A = Ar<T, EXACT>;
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const int sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
@@ -1087,14 +1136,14 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     T e = in.ex;
     const T dhz = c.jy ? A::dif(in.hz_i, in.hz_jm) : T(0);
     const T dhy = c.kz ? A::dif(in.hy_i, in.hy_km) : T(0);
-    p.coef.decode_k(3, in.r0, c.key, c.kez, c0, c1, c2, u1, u2);
+    p.coef.decode_k(3, in.r0, key, kez, c0, c1, c2, u1, u2);
     if (c.jy && c.kz) e = A::lin3(c0, e, c1, dhz, c2, dhy);
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 3, in.pa[0], in.ca[0],
                                            dhz, u1, dy, e);
     }
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 2, in.pb[0], in.cb[0],
                                            dhy, u2, dz, e);
@@ -1106,12 +1155,12 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     T e = in.ey;
     const T dhx = c.kz ? A::dif(in.hx_c, in.hx_km) : T(0);
     const T dhz = i >= 1 ? A::dif(in.hz_i, hz_p) : T(0);
-    p.coef.decode_k(4, in.r1, c.kez, in.kex, c0, c1, c2, u1, u2);
+    p.coef.decode_k(4, in.r1, kez, in.kex, c0, c1, c2, u1, u2);
     if (i >= 1 && c.kz) e = A::lin3(c0, e, c1, dhx, c2, dhz);
-    if (in.xf >= 0)
+    if ((F & kFX) && in.xf >= 0)
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 2, in.pa[1],
                                            in.ca[1], dhz, u2, dx, e);
-    if (cb.zf >= 0) {
+    if ((F & kFZ) && cb.zf >= 0) {
       const Face<T>& F = p.face[cb.zf];
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 3, in.pb[1], in.cb[1],
                                            dhx, u1, dz, e);
@@ -1123,12 +1172,12 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     T e = in.ez;
     const T dhy = i >= 1 ? A::dif(in.hy_i, hy_p) : T(0);
     const T dhx = c.jy ? A::dif(in.hx_c, in.hx_jm) : T(0);
-    p.coef.decode_k(5, in.r2, in.kex, c.key, c0, c1, c2, u1, u2);
+    p.coef.decode_k(5, in.r2, in.kex, key, c0, c1, c2, u1, u2);
     if (i >= 1 && c.jy) e = A::lin3(c0, e, c1, dhy, c2, dhx);
-    if (in.xf >= 0)
+    if ((F & kFX) && in.xf >= 0)
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 3, in.pa[2],
                                            in.ca[2], dhy, u1, dx, e);
-    if (cb.yf >= 0) {
+    if ((F & kFY) && cb.yf >= 0) {
       const Face<T>& F = p.face[cb.yf];
       cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 2, in.pb[2], in.cb[2],
                                            dhx, u2, dy, e);
@@ -1140,22 +1189,22 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
   hy_p = in.hy_i;
 }
 
-template <typename T, class C, bool EXACT, bool BPF>
+template <typename T, class C, bool EXACT, bool BPF, unsigned F = kFAll>
 __device__ __forceinline__ void e_band_range(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int a,
                                              int b, int ts, T& hz_p, T& hy_p) {
   if (a >= b) return;
   EBand<T, C> cur, nxt;
   if (!BPF) {
     for (int i = a; i < b; i++) {
-      e_band_load(p, c, cb, i, cur);
-      e_band_store<T, C, EXACT>(p, c, cb, i, ts, cur, hz_p, hy_p);
+      e_band_load<T, C, F>(p, c, cb, i, cur);
+      e_band_store<T, C, EXACT, F>(p, c, cb, i, ts, cur, hz_p, hy_p);
     }
     return;
   }
-  e_band_load(p, c, cb, a, cur);
+  e_band_load<T, C, F>(p, c, cb, a, cur);
   for (int i = a; i < b; i++) {
-    if (i + 1 < b) e_band_load(p, c, cb, i + 1, nxt);
-    e_band_store<T, C, EXACT>(p, c, cb, i, ts, cur, hz_p, hy_p);
+    if (i + 1 < b) e_band_load<T, C, F>(p, c, cb, i + 1, nxt);
+    e_band_store<T, C, EXACT, F>(p, c, cb, i, ts, cur, hz_p, hy_p);
     cur = nxt;
   }
 }
@@ -1182,6 +1231,43 @@ __device__ __forceinline__ void e_staged_range(const StepParams<float, TableCoef
   }
 }
 
+// Lean planes [xa, xb) of an E column (1 <= i < nx, no band, no source).
+template <typename T, class C, bool EXACT, int PF>
+__device__ __forceinline__ void e_lean_range(const StepParams<T, C>& p, const ECol<T>& c, int xa, int xb, T& hz_p,
+                                             T& hy_p) {
+  if constexpr (PF >= 3 && C::kTable) {
+    e_staged_range<PF>(p, c, xa, xb, hz_p, hy_p);
+  } else if (xa < xb) {
+    EIn<T, C> cur, nxt, nx2;
+    e_load(p, c, xa, cur);
+    if (PF == 2 && xa + 1 < xb) e_load(p, c, xa + 1, nxt);
+    for (int i = xa; i < xb; i++) {
+      if (PF == 1) {
+        if (i + 1 < xb) e_load(p, c, i + 1, nxt);
+      } else {
+        if (i + 2 < xb) e_load(p, c, i + 2, nx2);
+      }
+      e_store<T, C, EXACT>(p, c, i, cur, hz_p, hy_p);
+      cur = nxt;
+      if (PF == 2) nxt = nx2;
+    }
+  }
+}
+
+// Planes [i0, i1) of an E column in the band form (see h_tile_planes); the
+// edge ranges also hold the boundary planes i = 0 and i = nx.
+template <typename T, class C, bool EXACT, int PF, unsigned YZ>
+__device__ __forceinline__ void e_tile_planes(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i0,
+                                              int xa, int xb, int i1, int ts, T& hz_p, T& hy_p) {
+  constexpr bool BPF = BandForm<C>::kPrefetch;
+  e_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, i0, xa, ts, hz_p, hy_p);
+  if constexpr (YZ == 0)
+    e_lean_range<T, C, EXACT, PF>(p, c, xa, xb, hz_p, hy_p);
+  else
+    e_band_range<T, C, EXACT, BPF, YZ>(p, c, cb, xa, xb, ts, hz_p, hy_p);
+  e_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, xb, i1, ts, hz_p, hy_p);
+}
+
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
   const int k = bx * blockDim.x + threadIdx.x;
@@ -1205,8 +1291,11 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
   c.sx = source_columns(p.src, 0, j, k);
   c.sy = source_columns(p.src, 1, j, k);
   c.sz = source_columns(p.src, 2, j, k);
-  const bool lean_col = !valid || (c.yn < 0 && c.yp < 0 && c.zn < 0 && c.zp < 0 && !(c.sx | c.sy | c.sz));
-  const bool warp_lean = __all_sync(0xffffffffu, lean_col);
+  const bool ycol = c.yn >= 0 || c.yp >= 0, zcol = c.zn >= 0 || c.zp >= 0, scol = (c.sx | c.sy | c.sz) != 0;
+  const bool warp_lean = __all_sync(0xffffffffu, !valid || (!ycol && !zcol && !scol));
+  const bool warp_y = __any_sync(0xffffffffu, valid && ycol);
+  const bool warp_z = __any_sync(0xffffffffu, valid && zcol);
+  const bool warp_src = __any_sync(0xffffffffu, valid && scol);
   if (!valid) return;
   c.key = p.coef.invk(1, j);
   c.kez = p.coef.invk(2, k);
@@ -1215,45 +1304,35 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
   // carried x-neighbours: Hz(i-1,j,k), Hy(i-1,j,k)
   T hz_p = (i0 >= 1 && c.ey_ok) ? p.f.Hz[(i0 - 1) * ny * (nz + 1) + c.ob] : T(0);
   T hy_p = (i0 >= 1 && c.ez_ok) ? p.f.Hy[(i0 - 1) * (ny + 1) * nz + c.oa] : T(0);
-  // interior planes [xa, xb): 1 <= i < nx and outside both x bands
-  int xa = i1, xb = i1;
-  if (warp_lean) {
-    const int lo = p.face[0].nc > 0 ? p.face[0].e_start + p.face[0].nc : 1;
-    const int hi = p.face[1].nc > 0 ? p.face[1].e_start : nx;
-    xa = min(max(i0, max(lo, 1)), i1);
-    xb = max(xa, min(i1, min(hi, nx)));
-  }
-  ColBands cb{};
-  constexpr bool BPF = BandForm<C>::kPrefetch;
-  const bool band_form = BandForm<C>::kUse && p.bands_disjoint != 0;
-  if (band_form) {
+  // x-interior planes [xa, xb): 1 <= i < nx and outside both x bands
+  const int lo = p.face[0].nc > 0 ? p.face[0].e_start + p.face[0].nc : 1;
+  const int hi = p.face[1].nc > 0 ? p.face[1].e_start : nx;
+  const int xa = min(max(i0, max(lo, 1)), i1);
+  const int xb = max(xa, min(i1, min(hi, nx)));
+  if (BandForm<C>::kUse && p.bands_disjoint != 0) {
+    ColBands cb{};
     cb.yf = band_face(p.face, 1, j, true, cb.yci);
     cb.zf = band_face(p.face, 2, k, true, cb.zci);
-    e_band_range<T, C, EXACT, BPF>(p, c, cb, i0, xa, ts, hz_p, hy_p);
-  } else {
-    for (int i = i0; i < xa; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
-  }
-  if constexpr (PF >= 3 && C::kTable) {
-    e_staged_range<PF>(p, c, xa, xb, hz_p, hy_p);
-  } else if (xa < xb) {
-    EIn<T, C> cur, nxt, nx2;
-    e_load(p, c, xa, cur);
-    if (PF == 2 && xa + 1 < xb) e_load(p, c, xa + 1, nxt);
-    for (int i = xa; i < xb; i++) {
-      if (PF == 1) {
-        if (i + 1 < xb) e_load(p, c, i + 1, nxt);
-      } else {
-        if (i + 2 < xb) e_load(p, c, i + 2, nx2);
-      }
-      e_store<T, C, EXACT>(p, c, i, cur, hz_p, hy_p);
-      cur = nxt;
-      if (PF == 2) nxt = nx2;
+    if (warp_src) {  // source columns: the general form on every plane
+      e_band_range<T, C, EXACT, BandForm<C>::kPrefetch, kFAll>(p, c, cb, i0, i1, ts, hz_p, hy_p);
+    } else if (warp_y) {
+      if (warp_z)
+        e_tile_planes<T, C, EXACT, PF, kFY | kFZ>(p, c, cb, i0, xa, xb, i1, ts, hz_p, hy_p);
+      else
+        e_tile_planes<T, C, EXACT, PF, kFY>(p, c, cb, i0, xa, xb, i1, ts, hz_p, hy_p);
+    } else {
+      if (warp_z)
+        e_tile_planes<T, C, EXACT, PF, kFZ>(p, c, cb, i0, xa, xb, i1, ts, hz_p, hy_p);
+      else
+        e_tile_planes<T, C, EXACT, PF, 0>(p, c, cb, i0, xa, xb, i1, ts, hz_p, hy_p);
     }
+    return;
   }
-  if (band_form)
-    e_band_range<T, C, EXACT, BPF>(p, c, cb, xb, i1, ts, hz_p, hy_p);
-  else
-    for (int i = xb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  // plane-at-a-time form for the band planes; lean interior for lean warps
+  const int la = warp_lean ? xa : i1, lb = warp_lean ? xb : i1;
+  for (int i = i0; i < la; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
+  e_lean_range<T, C, EXACT, PF>(p, c, la, lb, hz_p, hy_p);
+  for (int i = lb; i < i1; i++) e_plane<T, C, EXACT, false>(p, c, i, ts, hz_p, hy_p);
 }
 
 template <typename T, class C, bool EXACT, int PF>
