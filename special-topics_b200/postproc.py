@@ -181,6 +181,24 @@ def farfield_cuts(acc: dict, g: Grid, ff: FarFieldBox) -> list:
     return out
 
 
-__all__ = ["time_to_freq", "dft_frequencies", "s11", "input_impedance", "port_s11", "radiated_power",
+def growth_onset(x, window: int = 250, factor: float = 10.0) -> int:
+    """First step at which the envelope of a port trace (max |x| over windows
+    of `window` steps) exceeds `factor` times its smallest value after the
+    pulse peak: where a run's late-time growth sets in (SURVEY 8(c)'s
+    stability check).  -1 when it never does."""
+    x = np.abs(np.asarray(x, dtype=np.float64))
+    nw = x.size // window
+    if nw < 3:
+        return -1
+    env = x[:nw * window].reshape(nw, window).max(axis=1)
+    lo = np.inf
+    for w in range(int(np.argmax(env)) + 1, nw):
+        lo = min(lo, env[w])
+        if lo > 0 and env[w] > factor * lo:
+            return w * window
+    return -1
+
+
+__all__ = ["time_to_freq", "growth_onset", "dft_frequencies", "s11", "input_impedance", "port_s11", "radiated_power",
            "directivity", "cut_angles", "to_db", "farfield_cuts", "FF_NAMES"]
 del C

@@ -57,7 +57,7 @@ def run_one(problem, precision: str, steps: int, device: int = 0, acc: str = "f6
         T, P = grid_2deg()
         radp, dth, dph = eng.farfield_post(T, P)
     return {"device_ms": ms, "wall_s": time.perf_counter() - t0, "s11_db": port["mag_dB"], "zin": port["zin"],
-            "radp": radp, "d": dth + dph}
+            "radp": radp, "d": dth + dph, "growth_onset_step": postproc.growth_onset(V)}
 
 
 def compare(ref: dict, other: dict) -> dict:
@@ -98,14 +98,15 @@ def main():
     ref = run_one(p64, "f64", args.steps)
     out = {"workload": scn["name"], "grid": [g.nx, g.ny, g.nz], "steps": args.steps,
            "far_field_freqs": int(p64.farfield.nFreq), "directions": int(grid_2deg()[0].size),
-           "f64": {"device_ms": ref["device_ms"]}}
+           "f64": {"device_ms": ref["device_ms"], "growth_onset_step": ref["growth_onset_step"]}}
     p32 = build_problem_from_scenario(scn, args.steps, per_cell=False)
     for name, acc in (("f32-table, FP64 accumulators", "f64"), ("f32-table, Kahan FP32 accumulators", "kahan-f32")):
         r32 = run_one(p32, "f32-table", args.steps, acc=acc)
-        out[name] = dict(compare(ref, r32), device_ms=r32["device_ms"])
+        out[name] = dict(compare(ref, r32), device_ms=r32["device_ms"], growth_onset_step=r32["growth_onset_step"])
     # FP32 fields with the reference's per-cell coefficient arrays
     r32 = run_one(p64, "f32", args.steps)
-    out["f32 per-cell, FP64 accumulators"] = dict(compare(ref, r32), device_ms=r32["device_ms"])
+    out["f32 per-cell, FP64 accumulators"] = dict(compare(ref, r32), device_ms=r32["device_ms"],
+                                                  growth_onset_step=r32["growth_onset_step"])
     text = json.dumps(out, indent=1)
     print(text, flush=True)
     if args.out:

@@ -117,3 +117,13 @@ def test_window_poles_and_tail_recover_two_modes():
     pol = ES.StopPolicy(pencil_orders=(4,))
     got = ES.best_tail(V, I, 2300, dt, pol)
     assert got is not None and got[2] < 1e-12
+
+
+def test_growth_onset_finds_late_growth():
+    from special_topics_b200 import postproc
+    n = np.arange(7000)
+    decay = np.exp(-n / 800.0) * np.cos(0.1 * n)
+    growth = 1e-6 * np.exp((n - 7000) / 300.0 + 12) * np.cos(2.5 * n)
+    assert postproc.growth_onset(decay) == -1
+    on = postproc.growth_onset(decay + growth)
+    assert 4000 < on < 7000
