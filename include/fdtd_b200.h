@@ -233,6 +233,14 @@ int fdtd_ctx_read_psi(fdtd_ctx* ctx, int faceId, int slot, double* host, long n)
  * cmxzp cmyzp cmxzn cmyzn), laid out [freq][point] like farfield.js:55. */
 int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, long n);
 
+/* Time-blocked surface DFT of an FP32 problem: the epilogue buffers each
+ * step's surface samples and every `steps` steps (and at the end of each run)
+ * they are accumulated at once, so the accumulators are read and written once
+ * per block instead of once per step.  0 (default) = every step; FP64
+ * problems keep the per-step form (their summation order is the reference's).
+ * Results match the per-step form to FP32 rounding. */
+int fdtd_ctx_set_dft_block(fdtd_ctx* ctx, int steps);
+
 /* Checkpoint / restore (SURVEY's fdtd_save_state / load_state; the reference
  * has none): the evolving state of a handle -- fields, Psi, port traces,
  * far-field accumulators, watchdog and step -- to and from a caller buffer

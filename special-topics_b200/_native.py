@@ -40,6 +40,7 @@ EXPORTS = (
     "fdtd_es_get_params", "fdtd_es_forward", "fdtd_es_loss_grad", "fdtd_es_set_data", "fdtd_es_train",
     "fdtd_es_member_inputs", "fdtd_es_predict_members", "fdtd_ctx_farfield_post",
     "fdtd_ctx_set_dft_accumulator", "fdtd_ctx_state_size", "fdtd_ctx_save_state", "fdtd_ctx_load_state",
+    "fdtd_ctx_set_dft_block",
 )
 
 
@@ -130,6 +131,7 @@ def lib() -> C.CDLL:
     L.fdtd_dft.argtypes = [dp, i, d, dp, i, d, dp, dp]
     L.fdtd_ctx_farfield_post.argtypes = [v, dp, dp, i, dp, dp, dp]
     L.fdtd_ctx_set_dft_accumulator.argtypes = [v, i]
+    L.fdtd_ctx_set_dft_block.argtypes = [v, i]
     L.fdtd_ctx_state_size.argtypes = [v, P(C.c_longlong)]
     L.fdtd_ctx_save_state.argtypes = [v, v, C.c_longlong]
     L.fdtd_ctx_load_state.argtypes = [v, v, C.c_longlong]

@@ -30,11 +30,12 @@ class Engine:
     """One problem resident on one GPU."""
 
     def __init__(self, problem: Problem, precision: str = "f64", device: int = 0, host_tables: bool = False,
-                 dft_accumulator: str = "f64"):
+                 dft_accumulator: str = "f64", dft_block: int = 0):
         """host_tables=True builds an FP32-table problem's ids with numpy
         (tables.build_tables, needs per-cell material arrays) instead of on the
         device (fdtd_ctx_build_material).  dft_accumulator "kahan-f32" keeps an
-        FP32 problem's far-field accumulators as compensated FP32 pairs."""
+        FP32 problem's far-field accumulators as compensated FP32 pairs; dft_block
+        > 0 accumulates the surface DFT once per that many steps (FP32)."""
         if dft_accumulator not in ("f64", "kahan-f32"):
             raise ValueError("dft_accumulator must be 'f64' or 'kahan-f32'")
         if precision not in PRECISIONS:
@@ -53,6 +54,8 @@ class Engine:
             self._upload()
             if dft_accumulator == "kahan-f32":
                 N.check(L.fdtd_ctx_set_dft_accumulator(h, 1))
+            if dft_block:
+                N.check(L.fdtd_ctx_set_dft_block(h, int(dft_block)))
         except Exception:
             self.close()
             raise

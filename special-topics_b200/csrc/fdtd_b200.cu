@@ -113,6 +113,9 @@ struct fdtd_ctx {
   double* acc = nullptr;
   std::vector<double> ffreq;  // far-field frequencies (Hz)
   int acc_kahan = 0;          // FP32 problems: compensated FP32 accumulator pairs instead of FP64
+  int dft_block = 0;          // FP32 problems: steps per time block of the surface DFT (0: every step)
+  float* dft_samples = nullptr;
+  int* d_dft_done = nullptr;
   long long ffsz[3] = {};
   long long ffoff[24] = {};
   void* ex0b = nullptr;
@@ -303,6 +306,9 @@ FarField dev_ff(const fdtd_ctx* c) {
   for (int a = 0; a < 24; a++) ff.off[a] = c->ffoff[a];
   for (int a = 0; a < 3; a++) ff.sz[a] = c->ffsz[a];
   ff.kahan = c->acc_kahan;
+  ff.block = c->dft_block;
+  ff.samples = c->dft_samples;
+  ff.done = c->d_dft_done;
   return ff;
 }
 
@@ -367,6 +373,8 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   p.dcell[2] = (T)c->dz;
   p.ichunk = c->ichunk;
   p.bands_disjoint = bands_disjoint(c);
+  p.dft_block = c->dft_block;
+  p.dft_done = c->d_dft_done;
   return p;
 }
 
@@ -413,6 +421,7 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   const unsigned mid_blocks = (unsigned)((plane + pr.n_i + 255) / 256);
   const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
   const unsigned epi_blocks = (unsigned)((nff + pr.n_v + 255) / 256);
+  const unsigned flush_blocks = (unsigned)((nff * std::max(c->nFreq, 1) + 255) / 256);
   auto kh = step_kernel<T, C, EXACT>(false, c->prefetch);
   auto ke = step_kernel<T, C, EXACT>(true, c->prefetch);
   size_t smem = 0;
@@ -428,6 +437,7 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
     ke<<<grd, blk, smem, c->stream>>>(p);
     if (tm) CK(cudaEventRecord(tm->ev[3], c->stream));
     if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, c->stream>>>(p.f, p.g, ff, pr, c->d_ts);
+    if (c->dft_block > 0) k_dft_flush<<<flush_blocks, 256, 0, c->stream>>>(ff, c->d_ts, -1);
     if (tm) {
       CK(cudaEventRecord(tm->ev[4], c->stream));
       CK(cudaEventSynchronize(tm->ev[4]));
@@ -563,6 +573,16 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
     CK(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+  }
+  if (c->dft_block > 0 && count > 0) {
+    // close the open block: accumulate what the run left buffered
+    const int upto = c->ts + count;
+    if (upto % c->dft_block != 0) {
+      const long long n = (c->ffsz[0] + c->ffsz[1] + c->ffsz[2]) * (long long)c->nFreq;
+      k_dft_flush<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(dev_ff(c), c->d_ts, upto);
+      CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(c->d_dft_done, &upto, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
   c->ts += count;
@@ -1277,8 +1297,31 @@ int fdtd_ctx_load_state(fdtd_ctx* c, const void* buf, long long bytes) {
   }
   const int dts = theirs.ts - 1;  // the device counter holds the index of the last step run
   CK(cudaMemcpyAsync(c->d_ts, &dts, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (c->d_dft_done)  // a saved state has no open DFT block
+    CK(cudaMemcpyAsync(c->d_dft_done, &theirs.ts, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->ts = theirs.ts;
+  return FDTD_OK;
+}
+
+int fdtd_ctx_set_dft_block(fdtd_ctx* c, int steps) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (steps < 0 || steps == 1 || steps > 1024) return fail(FDTD_ERR_BADARG, "DFT block of %d steps not in {0, 2..1024}", steps);
+  if (steps && c->prec == FDTD_PREC_F64) return fail(FDTD_ERR_BADARG, "FP64 problems keep the per-step DFT");
+  if (steps && c->nFreq == 0) return fail(FDTD_ERR_STATE, "no far field set up");
+  CK(cudaSetDevice(c->device));
+  if (steps) {
+    dfree(c, c->dft_samples);
+    c->dft_samples = nullptr;
+    const long long npts = c->ffsz[0] + c->ffsz[1] + c->ffsz[2];
+    int rc = dalloc(c, (void**)&c->dft_samples, sizeof(float) * (size_t)steps * npts * 8);
+    if (!rc && !c->d_dft_done) rc = dalloc(c, (void**)&c->d_dft_done, sizeof(int));
+    if (rc) return rc;
+    // every earlier step is already in the accumulators
+    CK(xfer(c, c->d_dft_done, &c->ts, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->dft_block = steps;
+  invalidate(c);
   return FDTD_OK;
 }
 
@@ -1666,6 +1709,8 @@ int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer
     if (ts + count > c->nsteps)
       return fail(FDTD_ERR_BADARG, "batch member %zu: running %d steps from step %d exceeds numberOfTimeSteps=%d", q,
                   count, ts, c->nsteps);
+    if (c->dft_block > 0)
+      return fail(FDTD_ERR_STATE, "batch member %zu uses the time-blocked DFT, which batches do not run", q);
     int rc = check_ready(c);
     if (!rc) rc = ensure_traces(c);
     if (!rc && c->prec == FDTD_PREC_F32_TABLE && c->table_dirty) rc = prepare_table(c, &c->tcoef);

@@ -77,7 +77,12 @@ struct FarField {
   long long off[24];
   long long sz[3];             // x-, y-, z-face point counts
   int kahan;                   // accumulators are FP32 (sum, compensation) pairs, not FP64
+  int block;                   // > 0: steps per time block (samples buffered, accumulated by k_dft_flush)
+  float* samples;              // [block][points][8] surface samples of the open block
+  const int* done;             // steps already accumulated
 };
+
+
 
 // Lumped source on the cell this thread owns (sources.js:271-288).
 template <typename T>
@@ -129,6 +134,24 @@ enum {
   CJYXP, CJZXP, CJYXN, CJZXN, CJXYP, CJZYP, CJXYN, CJZYN, CJXZP, CJYZP, CJXZN, CJYZN,
   CMYXP, CMZXP, CMYXN, CMZXN, CMXYP, CMZYP, CMXYN, CMZYN, CMXZP, CMYZP, CMXZN, CMYZN
 };
+
+// The 8 accumulator arrays a surface point feeds, in sample order, for the
+// x-face (0), y-face (1) and z-face (2) point pairs.
+__device__ __forceinline__ int sample_array(int group, int a) {
+  static constexpr int tab[3][8] = {{CMYXP, CMZXP, CJYXP, CJZXP, CMYXN, CMZXN, CJYXN, CJZXN},
+                                    {CMXYP, CMZYP, CJZYP, CJXYP, CMXYN, CMZYN, CJZYN, CJXYN},
+                                    {CMXZP, CMYZP, CJXZP, CJYZP, CMXZN, CMYZN, CJXZN, CJYZN}};
+  return tab[group][a];
+}
+
+// Time-blocked DFT: the epilogue stores a step's 8 samples per point in slot
+// ts % block; this writes them into the running accumulators.
+__device__ __forceinline__ void store_samples(const FarField& ff, long long t, int ts, const double* v) {
+  const long long npts = ff.sz[0] + ff.sz[1] + ff.sz[2];
+  float* s = ff.samples + ((long long)(ts % ff.block) * npts + t) * 8;
+#pragma unroll
+  for (int a = 0; a < 8; a++) s[a] = (float)v[a];
+}
 
 // One Kahan-compensated FP32 step: v = (sum, compensation), sum += x.
 __device__ __forceinline__ void kahan_add(float2* v, float x) {
@@ -187,6 +210,11 @@ __device__ __forceinline__ void epilogue_thread(const Fields<T>& f, const GridDi
     const double tmzxn = mul(0.5, add(EY(LI, j0, k0), EY(LI, j0, k0 + 1)));
     const double tjyxn = mul(0.25, add(add(add(HZ(LI, j0, k0), HZ(LI, j0, k0 + 1)), HZ(LI - 1, j0, k0)), HZ(LI - 1, j0, k0 + 1)));
     const double tjzxn = mul(-0.25, add(add(add(HY(LI, j0, k0), HY(LI, j0 + 1, k0)), HY(LI - 1, j0, k0)), HY(LI - 1, j0 + 1, k0)));
+    if (ff.block) {  // time-blocked: buffer the samples, k_dft_flush accumulates them
+      const double v[8] = {tmyxp, tmzxp, tjyxp, tjzxp, tmyxn, tmzxn, tjyxn, tjzxn};
+      store_samples(ff, t, ts, v);
+      return;
+    }
     for (int m = 0; m < ff.nFreq; m++) {
       const long long p = (long long)m * ff.sz[0] + t;
       const double ch = ph[4 * m], sh = ph[4 * m + 1], ce = ph[4 * m + 2], se = ph[4 * m + 3];
@@ -211,6 +239,11 @@ __device__ __forceinline__ void epilogue_thread(const Fields<T>& f, const GridDi
     const double tmzyn = mul(-0.5, add(EX(i0, LJ, k0), EX(i0, LJ, k0 + 1)));
     const double tjzyn = mul(0.25, add(add(add(HX(i0, LJ, k0), HX(i0 + 1, LJ, k0)), HX(i0, LJ - 1, k0)), HX(i0 + 1, LJ - 1, k0)));
     const double tjxyn = mul(-0.25, add(add(add(HZ(i0, LJ, k0), HZ(i0, LJ, k0 + 1)), HZ(i0, LJ - 1, k0)), HZ(i0, LJ - 1, k0 + 1)));
+    if (ff.block) {  // time-blocked: buffer the samples, k_dft_flush accumulates them
+      const double v[8] = {tmxyp, tmzyp, tjzyp, tjxyp, tmxyn, tmzyn, tjzyn, tjxyn};
+      store_samples(ff, t, ts, v);
+      return;
+    }
     for (int m = 0; m < ff.nFreq; m++) {
       const long long p = (long long)m * ff.sz[1] + q;
       const double ch = ph[4 * m], sh = ph[4 * m + 1], ce = ph[4 * m + 2], se = ph[4 * m + 3];
@@ -235,6 +268,11 @@ __device__ __forceinline__ void epilogue_thread(const Fields<T>& f, const GridDi
     const double tmyzn = mul(0.5, add(EX(i0, j0, LK), EX(i0, j0 + 1, LK)));
     const double tjxzn = mul(0.25, add(add(add(HY(i0, j0, LK), HY(i0, j0 + 1, LK)), HY(i0, j0, LK - 1)), HY(i0, j0 + 1, LK - 1)));
     const double tjyzn = mul(-0.25, add(add(add(HX(i0, j0, LK), HX(i0 + 1, j0, LK)), HX(i0, j0, LK - 1)), HX(i0 + 1, j0, LK - 1)));
+    if (ff.block) {  // time-blocked: buffer the samples, k_dft_flush accumulates them
+      const double v[8] = {tmxzp, tmyzp, tjxzp2, tjxzp, tmxzn, tmyzn, tjxzn, tjyzn};
+      store_samples(ff, t, ts, v);
+      return;
+    }
     for (int m = 0; m < ff.nFreq; m++) {
       const long long p = (long long)m * ff.sz[2] + q;
       const double ch = ph[4 * m], sh = ph[4 * m + 1], ce = ph[4 * m + 2], se = ph[4 * m + 3];
@@ -272,6 +310,50 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_epilogue(Fields<T> f, GridDims g, FarField ff, Probes probes,
                                                   const int* ts_ptr) {
   epilogue_thread<T>(f, g, ff, probes, ts_ptr, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Accumulates the buffered samples of steps [*ff.done, upto) into the
+// running DFT: one thread per (surface point pair, frequency), steps in
+// order.  upto < 0: flush only when the step just finished closes a block
+// (upto = ts + 1 then), so the launch can sit in every step of a graph.
+__global__ void __launch_bounds__(256) k_dft_flush(FarField ff, const int* ts_ptr, int upto) {
+  const long long npts = ff.sz[0] + ff.sz[1] + ff.sz[2];
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts * ff.nFreq) return;
+  if (upto < 0) {
+    const int ts = *ts_ptr;
+    if ((ts + 1) % ff.block != 0) return;
+    upto = ts + 1;
+  }
+  const int from = *ff.done;
+  const long long t = q % npts;
+  const int m = (int)(q / npts);
+  const int group = t < ff.sz[0] ? 0 : t < ff.sz[0] + ff.sz[1] ? 1 : 2;
+  const long long p = (long long)m * ff.sz[group] + (group == 0 ? t : group == 1 ? t - ff.sz[0] : t - ff.sz[0] - ff.sz[1]);
+  for (int a = 0; a < 8; a++) {
+    const int arr = sample_array(group, a);
+    const int e = arr >= CMYXP ? 2 : 0;  // magnetic currents take the E-time phasor
+    double* re = ff.acc + ff.off[arr] + p;
+    double* im = re + ff.nFreq * ff.sz[group];
+    if (ff.kahan) {
+      for (int s = from; s < upto; s++) {
+        const double* ph = ff.ph + ((long long)s * ff.nFreq + m) * 4 + e;
+        const float v = ff.samples[((long long)(s % ff.block) * npts + t) * 8 + a];
+        kahan_add(reinterpret_cast<float2*>(re), __fmul_rn((float)ph[0], v));
+        kahan_add(reinterpret_cast<float2*>(im), __fmul_rn((float)ph[1], v));
+      }
+    } else {
+      double r = *re, i = *im;
+      for (int s = from; s < upto; s++) {
+        const double* ph = ff.ph + ((long long)s * ff.nFreq + m) * 4 + e;
+        const double v = ff.samples[((long long)(s % ff.block) * npts + t) * 8 + a];
+        r += ph[0] * v;
+        i += ph[1] * v;
+      }
+      *re = r;
+      *im = i;
+    }
+  }
 }
 
 }  // namespace fdtd

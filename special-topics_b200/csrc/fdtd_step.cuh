@@ -157,6 +157,8 @@ struct StepParams {
   T dcell[3];
   int ichunk;  // x planes per thread
   int bands_disjoint;  // per axis, no position lies in both CPML bands (H and E)
+  int dft_block;       // time-blocked surface DFT: steps per block (0: per step)
+  int* dft_done;       // steps the blocked DFT has accumulated
 };
 
 // Band of a face that contains `pos` (H: m band, E: e band): ci or -1.
@@ -790,8 +792,12 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
 
 template <typename T, class C, bool EXACT, int PF>
 __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value) k_step_h(StepParams<T, C> p) {
-  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
-    *p.ts += 1;  // first kernel of a step advances the device step counter
+  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    const int ts = *p.ts + 1;  // first kernel of a step advances the device step counter
+    *p.ts = ts;
+    // a block boundary: the previous block was flushed at the end of step ts - 1
+    if (p.dft_block > 0 && ts % p.dft_block == 0) *p.dft_done = ts;
+  }
   step_h_tile<T, C, EXACT, PF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 

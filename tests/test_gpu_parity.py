@@ -322,3 +322,35 @@ def test_state_checkpoint_resumes_bit_identically(precision):
     with Engine(other, precision) as c:
         with pytest.raises(N.FdtdError):
             c.load_state(state)
+
+
+@pytest.mark.parametrize("acc", ["f64", "kahan-f32"])
+def test_time_blocked_dft_matches_per_step(acc):
+    """Surface samples buffered for 16 steps and accumulated at once give the
+    per-step accumulators to FP32 rounding, across graph replays, partial
+    blocks at run ends and a checkpoint/restore in the middle of a block."""
+    scn = small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3), steps=200, nff=3)
+    p = build_problem_from_scenario(scn, 200, per_cell=False)
+    with Engine(p, "f32-table", dft_accumulator=acc) as a, \
+            Engine(p, "f32-table", dft_accumulator=acc, dft_block=16) as b:
+        for n in (23, 64, 41, 5):
+            a.run(n)
+            b.run(n)
+        state = b.save_state()
+        fa, fb = a.farfield(), b.farfield()
+        for name in FF_NAMES:
+            for q in range(2):
+                scale = np.abs(fa[name][q]).max() + 1e-30
+                assert np.abs(fa[name][q] - fb[name][q]).max() <= 1e-5 * scale, name
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        a.run(67)
+        with Engine(p, "f32-table", dft_accumulator=acc, dft_block=16) as c:
+            c.load_state(state)
+            c.run(67)
+            fa, fc = a.farfield(), c.farfield()
+            for name in FF_NAMES:
+                scale = np.abs(fa[name][0]).max() + 1e-30
+                assert np.abs(fa[name][0] - fc[name][0]).max() <= 1e-5 * scale, name
+    with Engine(build_problem_from_scenario(scn, 200), "f64") as d:
+        with pytest.raises(N.FdtdError):
+            N.check(N.lib().fdtd_ctx_set_dft_block(d._h, 16))
