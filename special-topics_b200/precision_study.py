@@ -45,12 +45,12 @@ def grid_2deg():
     return T.ravel(), P.ravel()
 
 
-def run_one(problem, precision: str, steps: int, device: int = 0, acc: str = "f64") -> dict:
+def run_one(problem, precision: str, steps: int, device: int = 0, acc: str = "f64", block: int = 0) -> dict:
     from special_topics_b200 import postproc
     from special_topics_b200.backend import Engine
     freqs = np.linspace(1e9, 4e9, 301)
     t0 = time.perf_counter()
-    with Engine(problem, precision, device=device, dft_accumulator=acc) as eng:
+    with Engine(problem, precision, device=device, dft_accumulator=acc, dft_block=block) as eng:
         ms = eng.run_timed(steps)
         V, I = eng.voltages()[0], eng.currents()[0]
         port = postproc.port_s11(V, I, problem.grid.dt, freqs, 50.0)
@@ -100,8 +100,10 @@ def main():
            "far_field_freqs": int(p64.farfield.nFreq), "directions": int(grid_2deg()[0].size),
            "f64": {"device_ms": ref["device_ms"], "growth_onset_step": ref["growth_onset_step"]}}
     p32 = build_problem_from_scenario(scn, args.steps, per_cell=False)
-    for name, acc in (("f32-table, FP64 accumulators", "f64"), ("f32-table, Kahan FP32 accumulators", "kahan-f32")):
-        r32 = run_one(p32, "f32-table", args.steps, acc=acc)
+    for name, acc, block in (("f32-table, FP64 accumulators", "f64", 0),
+                             ("f32-table, Kahan FP32 accumulators", "kahan-f32", 0),
+                             ("f32-table, FP64 accumulators, DFT blocked by 16 steps", "f64", 16)):
+        r32 = run_one(p32, "f32-table", args.steps, acc=acc, block=block)
         out[name] = dict(compare(ref, r32), device_ms=r32["device_ms"], growth_onset_step=r32["growth_onset_step"])
     # FP32 fields with the reference's per-cell coefficient arrays
     r32 = run_one(p64, "f32", args.steps)
