@@ -1536,7 +1536,8 @@ struct fdtd_batch {
   BatchBlock* d_epi = nullptr;
   BatchCtl* d_ctl = nullptr;
   std::vector<BatchTile> tiles;
-  std::vector<BatchBlock> mid, epi;
+  std::vector<BatchBlock> mid, epi, flush;
+  BatchBlock* d_flush = nullptr;
   int grid_h = 0, grid_e = 0;  // persistent grid sizes
   cudaGraphExec_t graph = nullptr;
 };
@@ -1583,7 +1584,7 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
   const int n = (int)b->m.size();
   std::vector<unsigned char> host((size_t)n * sizeof(In), 0);
   std::vector<BatchTile> tiles;
-  std::vector<BatchBlock> mid, epi;
+  std::vector<BatchBlock> mid, epi, flush;
   for (int q = 0; q < n; q++) {
     fdtd_ctx* c = b->m[q];
     In in;
@@ -1606,6 +1607,8 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
     for (long long s = 0; s < (nmid + 255) / 256; s++) mid.push_back(BatchBlock{q, (int)s});
     const long long nff = (c->nFreq > 0) ? c->ffsz[0] + c->ffsz[1] + c->ffsz[2] : 0;
     for (long long s = 0; s < (nff + in.pr.n_v + 255) / 256; s++) epi.push_back(BatchBlock{q, (int)s});
+    if (c->dft_block > 0)
+      for (long long s = 0; s < (nff * c->nFreq + 255) / 256; s++) flush.push_back(BatchBlock{q, (int)s});
   }
   if (tiles.size() > (size_t)INT32_MAX) return fail(FDTD_ERR_BADARG, "batch has too many tiles");
   if (!b->d_inst || b->inst_size != sizeof(In)) {
@@ -1621,14 +1624,16 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
   };
   const bool same_tiles = tiles.size() == b->tiles.size() &&
                           (tiles.empty() || !memcmp(tiles.data(), b->tiles.data(), tiles.size() * sizeof(BatchTile)));
-  if (!same_tiles || !same(mid, b->mid) || !same(epi, b->epi) || !b->d_tiles) {
+  if (!same_tiles || !same(mid, b->mid) || !same(epi, b->epi) || !same(flush, b->flush) || !b->d_tiles) {
     batch_drop_graph(b);
     b->tiles.swap(tiles);
     b->mid.swap(mid);
     b->epi.swap(epi);
+    b->flush.swap(flush);
     int rc = upload_vec(b, &b->d_tiles, b->tiles);
     if (!rc) rc = upload_vec(b, &b->d_mid, b->mid);
     if (!rc) rc = upload_vec(b, &b->d_epi, b->epi);
+    if (!rc) rc = upload_vec(b, &b->d_flush, b->flush);
     if (rc) return rc;
   }
   // persistent grids: as many blocks as fit on the device at once
@@ -1665,11 +1670,14 @@ int batch_enqueue(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
     if (tm) CK(cudaEventRecord(tm->ev[0], b->stream));
     kh<<<gh, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
     if (tm) CK(cudaEventRecord(tm->ev[1], b->stream));
-    k_batch_mid<T, C, EXACT><<<(unsigned)b->mid.size(), 256, 0, b->stream>>>(in, b->d_mid, b->d_ctl);
+    k_batch_mid<T, C, EXACT><<<(unsigned)b->mid.size(), 256, 0, b->stream>>>(in, b->d_mid, b->d_ctl,
+                                                                             (int)b->m.size());
     if (tm) CK(cudaEventRecord(tm->ev[2], b->stream));
     ke<<<ge, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
     if (tm) CK(cudaEventRecord(tm->ev[3], b->stream));
     if (!b->epi.empty()) k_batch_epilogue<T, C><<<(unsigned)b->epi.size(), 256, 0, b->stream>>>(in, b->d_epi);
+    if (!b->flush.empty())
+      k_batch_flush<T, C><<<(unsigned)b->flush.size(), 256, 0, b->stream>>>(in, b->d_flush, -1);
     if (tm) {
       CK(cudaEventRecord(tm->ev[4], b->stream));
       CK(cudaEventSynchronize(tm->ev[4]));
@@ -1694,6 +1702,25 @@ int batch_prepare_any(fdtd_batch* b) {
   return batch_prepare<float, TableCoef, false>(b, coef_table);
 }
 
+// Closes the members' open DFT blocks at the end of a run reaching `upto`.
+template <typename T, class C>
+int batch_close_blocks(fdtd_batch* b, int upto) {
+  if (b->flush.empty()) return FDTD_OK;
+  k_batch_flush<T, C><<<(unsigned)b->flush.size(), 256, 0, b->stream>>>((const Instance<T, C>*)b->d_inst, b->d_flush,
+                                                                        upto);
+  CK(cudaGetLastError());
+  for (fdtd_ctx* c : b->m)
+    if (c->dft_block > 0) CK(cudaMemcpyAsync(c->d_dft_done, &upto, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return FDTD_OK;
+}
+
+int batch_close_any(fdtd_batch* b, int upto) {
+  if (b->prec == FDTD_PREC_F64) return batch_close_blocks<double, ArrayCoef<double>>(b, upto);
+  if (b->prec == FDTD_PREC_F32) return batch_close_blocks<float, ArrayCoef<float>>(b, upto);
+  return batch_close_blocks<float, TableCoef>(b, upto);
+}
+
 int batch_enqueue_any(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
   if (b->prec == FDTD_PREC_F64) return batch_enqueue<double, ArrayCoef<double>, true>(b, count, tm);
   if (b->prec == FDTD_PREC_F32) return batch_enqueue<float, ArrayCoef<float>, true>(b, count, tm);
@@ -1709,8 +1736,6 @@ int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer
     if (ts + count > c->nsteps)
       return fail(FDTD_ERR_BADARG, "batch member %zu: running %d steps from step %d exceeds numberOfTimeSteps=%d", q,
                   count, ts, c->nsteps);
-    if (c->dft_block > 0)
-      return fail(FDTD_ERR_STATE, "batch member %zu uses the time-blocked DFT, which batches do not run", q);
     int rc = check_ready(c);
     if (!rc) rc = ensure_traces(c);
     if (!rc && c->prec == FDTD_PREC_F32_TABLE && c->table_dirty) rc = prepare_table(c, &c->tcoef);
@@ -1762,6 +1787,10 @@ int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer
     CK(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+  }
+  if (count > 0) {
+    rc = batch_close_any(b, ts + count);
+    if (rc) return rc;
   }
   // hand the shared step counter back to every member
   for (fdtd_ctx* c : b->m) CK(cudaMemcpyAsync(c->d_ts, &b->d_ctl->ts, sizeof(int), cudaMemcpyDeviceToDevice, b->stream));
@@ -1820,6 +1849,7 @@ void fdtd_batch_free(fdtd_batch* b) {
   cudaFree(b->d_tiles);
   cudaFree(b->d_mid);
   cudaFree(b->d_epi);
+  cudaFree(b->d_flush);
   cudaFree(b->d_ctl);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

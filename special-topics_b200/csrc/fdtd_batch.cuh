@@ -97,10 +97,15 @@ __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value)
 // the E launch after it has not started.
 template <typename T, class C, bool EXACT>
 __global__ void __launch_bounds__(256)
-    k_batch_mid(const Instance<T, C>* __restrict__ inst, const BatchBlock* __restrict__ blocks, BatchCtl* ctl) {
+    k_batch_mid(const Instance<T, C>* __restrict__ inst, const BatchBlock* __restrict__ blocks, BatchCtl* ctl,
+                int ninst) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->next[0] = 0;
     ctl->next[1] = 0;
+    // time-blocked DFT: at a block boundary the previous block has been flushed
+    const int ts = ctl->ts;
+    for (int q = 0; q < ninst; q++)
+      if (inst[q].sp.dft_block > 0 && ts % inst[q].sp.dft_block == 0) *inst[q].sp.dft_done = ts;
   }
   const BatchBlock b = blocks[blockIdx.x];
   const Instance<T, C>& in = inst[b.inst];
@@ -114,6 +119,15 @@ __global__ void __launch_bounds__(256)
   const BatchBlock b = blocks[blockIdx.x];
   const Instance<T, C>& in = inst[b.inst];
   epilogue_thread<T>(in.sp.f, in.sp.g, in.ff, in.pr, in.sp.ts, (long long)b.local * blockDim.x + threadIdx.x);
+}
+
+// Time-blocked DFT flush of every member (see k_dft_flush).
+template <typename T, class C>
+__global__ void __launch_bounds__(256)
+    k_batch_flush(const Instance<T, C>* __restrict__ inst, const BatchBlock* __restrict__ blocks, int upto) {
+  const BatchBlock b = blocks[blockIdx.x];
+  const Instance<T, C>& in = inst[b.inst];
+  dft_flush_thread(in.ff, in.sp.ts, upto, (long long)b.local * blockDim.x + threadIdx.x);
 }
 
 }  // namespace fdtd

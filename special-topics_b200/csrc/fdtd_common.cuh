@@ -316,10 +316,10 @@ __global__ void __launch_bounds__(256) k_epilogue(Fields<T> f, GridDims g, FarFi
 // running DFT: one thread per (surface point pair, frequency), steps in
 // order.  upto < 0: flush only when the step just finished closes a block
 // (upto = ts + 1 then), so the launch can sit in every step of a graph.
-__global__ void __launch_bounds__(256) k_dft_flush(FarField ff, const int* ts_ptr, int upto) {
+__device__ __forceinline__ void dft_flush_thread(const FarField& ff, const int* ts_ptr, int upto, long long q) {
   const long long npts = ff.sz[0] + ff.sz[1] + ff.sz[2];
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= npts * ff.nFreq) return;
+  if (ff.block <= 0 || q >= npts * ff.nFreq) return;
+  if (upto >= 0 && upto % ff.block == 0) return;  // closed by the flush inside its last step
   if (upto < 0) {
     const int ts = *ts_ptr;
     if ((ts + 1) % ff.block != 0) return;
@@ -354,6 +354,10 @@ __global__ void __launch_bounds__(256) k_dft_flush(FarField ff, const int* ts_pt
       *im = i;
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_dft_flush(FarField ff, const int* ts_ptr, int upto) {
+  dft_flush_thread(ff, ts_ptr, upto, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace fdtd

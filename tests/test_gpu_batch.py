@@ -165,3 +165,24 @@ def test_batch_watchdog_names_the_member():
     finally:
         for e in engs:
             e.close()
+
+
+def test_batch_with_time_blocked_dft_matches_solo_runs():
+    probs = [build_problem_from_scenario(s, 90, per_cell=False)
+             for s in (small_scenario(1, "xp"), small_scenario(3, "zp", ncpml=(5, 4, 3, 3, 4, 5)))]
+    solo = []
+    for p in probs:
+        with Engine(p, "f32-table", dft_block=16) as e:
+            e.run(70)
+            e.run(20)
+            solo.append(_state(e))
+    engs = [Engine(p, "f32-table", dft_block=16) for p in probs]
+    try:
+        with Batch(engs) as b:
+            b.run(70)
+            b.run(20)
+        for q, e in enumerate(engs):
+            _assert_same(solo[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
