@@ -181,15 +181,25 @@ __device__ __forceinline__ void cpml_apply(const C& coef, const Face<T>& F, int 
 }
 
 // The same correction as cpml_apply with Psi (and CPsi, per-cell layouts)
-// loaded earlier: b and a come from the face's 1-D profiles (cache resident).
-template <typename T, class C, bool EXACT, bool ELECTRIC>
-__device__ __forceinline__ void cpml_apply_loaded(const C& coef, const Face<T>& F, int ci, int pi, int slot, T psi,
-                                                  T cp, T drive, T u, T dcell, T& v) {
-  const T b = ELECTRIC ? F.b_e[ci] : F.b_m[ci];
-  const T a = ELECTRIC ? F.a_e[ci] : F.a_m[ci];
+// loaded earlier and the band cell's profile values b and a held in
+// registers: Psi = b Psi + a drive is stored at P, then v += CPsi Psi.
+template <typename T, class C, bool EXACT>
+__device__ __forceinline__ void cpml_fold(const C& coef, T* P, T b, T a, T psi, T cp, T drive, T u, T dcell, T& v) {
   const T ps = Ar<T, EXACT>::lin2(b, psi, a, drive);
-  F.psi[slot][pi] = ps;
+  *P = ps;
   v = Ar<T, EXACT>::axpy(v, coef.cpsi_use(cp, u, dcell), ps);
+}
+
+// Profile values b, a of band cell ci of face f (H: m profiles, E: e
+// profiles); zero when f < 0.
+template <typename T, bool ELECTRIC>
+__device__ __forceinline__ void band_profile(const Face<T>* face, int f, int ci, T& b, T& a) {
+  b = T(0);
+  a = T(0);
+  if (f < 0) return;
+  const Face<T>& F = face[f];
+  b = __ldg((ELECTRIC ? F.b_e : F.b_m) + ci);
+  a = __ldg((ELECTRIC ? F.a_e : F.a_m) + ci);
 }
 
 // Face of axis `a` (0..2) whose band holds `pos`, and the band cell; -1 if none.
@@ -203,10 +213,23 @@ __device__ __forceinline__ int band_face(const Face<T>* face, int a, int pos, bo
 }
 
 // Column band state shared by the band loads and stores: y and z faces of the
-// column (-1 if none) and the band cells.
+// column (-1 if none), the band cells and their profile values b, a.
+template <typename T>
 struct ColBands {
   int yf, yci, zf, zci;
+  T yb, ya, zb, za;
 };
+
+// Band state of column (j, k) for the H (ELECTRIC = false) or E update.
+template <typename T, bool ELECTRIC>
+__device__ __forceinline__ ColBands<T> col_bands(const Face<T>* face, int j, int k) {
+  ColBands<T> cb;
+  cb.yf = band_face(face, 1, j, ELECTRIC, cb.yci);
+  cb.zf = band_face(face, 2, k, ELECTRIC, cb.zci);
+  band_profile<T, ELECTRIC>(face, cb.yf, cb.yci, cb.yb, cb.ya);
+  band_profile<T, ELECTRIC>(face, cb.zf, cb.zci, cb.zb, cb.za);
+  return cb;
+}
 
 // Source boxes that contain this thread's (j, k) for component `comp` (bit mask).
 template <typename T>
@@ -384,6 +407,7 @@ struct HBand {
   HIn<T, C> v;          // field values and coefficient raws
   float kmx;            // 1/kappa_m at plane i
   int xf, xci;          // x band of plane i: face and cell, or -1
+  T xb, xa;             // its profile values
   T pa[3], pb[3];       // Psi of the first / second correcting face of Hx, Hy, Hz
   T ca[3], cb[3];       // their CPsi (per-cell layouts; unused with tables)
 };
@@ -395,13 +419,14 @@ struct HBand {
 constexpr unsigned kFX = 1, kFY = 2, kFZ = 4, kFAll = 7;
 
 template <typename T, class C, unsigned F = kFAll>
-__device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
+__device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCol<T>& c, const ColBands<T>& cb, int i,
                                             HBand<T, C>& in) {
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
   const Fields<T>& f = p.f;
   if (F & kFX) {
     in.xf = band_face(p.face, 0, i, false, in.xci);
+    band_profile<T, false>(p.face, in.xf, in.xci, in.xb, in.xa);
     in.kmx = p.coef.invk(3, i);
   } else {
     in.xf = -1;
@@ -417,16 +442,16 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
     in.v.ez_jp = f.Ez[i * sHyEz + c.oa + nz];
     in.v.r0 = p.coef.fetch(0, idx);
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      const int pi = (i * F.nc + cb.yci) * nz + c.k;
-      in.pa[0] = F.psi[0][pi];
-      in.ca[0] = p.coef.cpsi_fetch(F, 0, pi);
+      const Face<T>& fc = p.face[cb.yf];
+      const int pi = (i * fc.nc + cb.yci) * nz + c.k;
+      in.pa[0] = fc.psi[0][pi];
+      in.ca[0] = p.coef.cpsi_fetch(fc, 0, pi);
     }
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      const int pi = (i * ny + c.j) * F.nc + cb.zci;
-      in.pb[0] = F.psi[0][pi];
-      in.cb[0] = p.coef.cpsi_fetch(F, 0, pi);
+      const Face<T>& fc = p.face[cb.zf];
+      const int pi = (i * ny + c.j) * fc.nc + cb.zci;
+      in.pb[0] = fc.psi[0][pi];
+      in.cb[0] = p.coef.cpsi_fetch(fc, 0, pi);
     }
   }
   if (i < nx) {
@@ -439,16 +464,16 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
       in.v.ez_n = f.Ez[idx + sHyEz];
       in.v.r1 = p.coef.fetch(1, idx);
       if (in.xf >= 0) {
-        const Face<T>& F = p.face[in.xf];
+        const Face<T>& fc = p.face[in.xf];
         const int pi = in.xci * sHyEz + c.oa;
-        in.pa[1] = F.psi[0][pi];
-        in.ca[1] = p.coef.cpsi_fetch(F, 0, pi);
+        in.pa[1] = fc.psi[0][pi];
+        in.ca[1] = p.coef.cpsi_fetch(fc, 0, pi);
       }
       if ((F & kFZ) && cb.zf >= 0) {
-        const Face<T>& F = p.face[cb.zf];
-        const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
-        in.pb[1] = F.psi[1][pi];
-        in.cb[1] = p.coef.cpsi_fetch(F, 1, pi);
+        const Face<T>& fc = p.face[cb.zf];
+        const int pi = (i * nyp1 + c.j) * fc.nc + cb.zci;
+        in.pb[1] = fc.psi[1][pi];
+        in.cb[1] = p.coef.cpsi_fetch(fc, 1, pi);
       }
     }
     if (c.hz_ok) {
@@ -458,16 +483,16 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
       in.v.ey_n = f.Ey[idx + sHzEy];
       in.v.r2 = p.coef.fetch(2, idx);
       if (in.xf >= 0) {
-        const Face<T>& F = p.face[in.xf];
+        const Face<T>& fc = p.face[in.xf];
         const int pi = in.xci * sHzEy + c.ob;
-        in.pa[2] = F.psi[1][pi];
-        in.ca[2] = p.coef.cpsi_fetch(F, 1, pi);
+        in.pa[2] = fc.psi[1][pi];
+        in.ca[2] = p.coef.cpsi_fetch(fc, 1, pi);
       }
       if ((F & kFY) && cb.yf >= 0) {
-        const Face<T>& F = p.face[cb.yf];
-        const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
-        in.pb[2] = F.psi[1][pi];
-        in.cb[2] = p.coef.cpsi_fetch(F, 1, pi);
+        const Face<T>& fc = p.face[cb.yf];
+        const int pi = (i * fc.nc + cb.yci) * nzp1 + c.k;
+        in.pb[2] = fc.psi[1][pi];
+        in.cb[2] = p.coef.cpsi_fetch(fc, 1, pi);
       }
     }
   }
@@ -476,7 +501,7 @@ __device__ __forceinline__ void h_band_load(const StepParams<T, C>& p, const HCo
 // h_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
 // arithmetic in the identical order.
 template <typename T, class C, bool EXACT, unsigned F = kFAll>
-__device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i,
+__device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HCol<T>& c, const ColBands<T>& cb, int i,
                                              const HBand<T, C>& in, T& ez_c, T& ey_c) {
   const float kmy = (F & kFY) ? c.kmy : 1.f, kmz = (F & kFZ) ? c.kmz : 1.f;
   using A = Ar<T, EXACT>;
@@ -491,14 +516,14 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
     p.coef.decode_k(0, in.v.r0, kmz, kmy, c0, c1, c2, u1, u2);
     T h = A::lin3(c0, in.v.hx, c1, dey, c2, dez);
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 0, in.pa[0], in.ca[0],
-                                            dez, u2, dy, h);
+      const Face<T>& fc = p.face[cb.yf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[0] + (i * fc.nc + cb.yci) * nz + c.k, cb.yb, cb.ya, in.pa[0], in.ca[0], dez,
+                             u2, dy, h);
     }
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 0, in.pb[0], in.cb[0],
-                                            dey, u1, dz, h);
+      const Face<T>& fc = p.face[cb.zf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[0] + (i * ny + c.j) * fc.nc + cb.zci, cb.zb, cb.za, in.pb[0], in.cb[0], dey,
+                             u1, dz, h);
     }
     f.Hx[i * sHx + c.oa] = h;
   }
@@ -509,12 +534,12 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
       p.coef.decode_k(1, in.v.r1, in.kmx, kmz, c0, c1, c2, u1, u2);
       T h = A::lin3(c0, in.v.hy, c1, dez, c2, dex);
       if ((F & kFX) && in.xf >= 0)
-        cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 0, in.pa[1],
-                                              in.ca[1], dez, u1, dx, h);
+        cpml_fold<T, C, EXACT>(p.coef, p.face[in.xf].psi[0] + in.xci * sHyEz + c.oa, in.xb, in.xa, in.pa[1], in.ca[1],
+                               dez, u1, dx, h);
       if ((F & kFZ) && cb.zf >= 0) {
-        const Face<T>& F = p.face[cb.zf];
-        cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 1, in.pb[1],
-                                              in.cb[1], dex, u2, dz, h);
+        const Face<T>& fc = p.face[cb.zf];
+        cpml_fold<T, C, EXACT>(p.coef, fc.psi[1] + (i * nyp1 + c.j) * fc.nc + cb.zci, cb.zb, cb.za, in.pb[1], in.cb[1],
+                               dex, u2, dz, h);
       }
       f.Hy[i * sHyEz + c.oa] = h;
     }
@@ -524,12 +549,12 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
       p.coef.decode_k(2, in.v.r2, kmy, in.kmx, c0, c1, c2, u1, u2);
       T h = A::lin3(c0, in.v.hz, c1, dex, c2, dey);
       if ((F & kFX) && in.xf >= 0)
-        cpml_apply_loaded<T, C, EXACT, false>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 1, in.pa[2],
-                                              in.ca[2], dey, u2, dx, h);
+        cpml_fold<T, C, EXACT>(p.coef, p.face[in.xf].psi[1] + in.xci * sHzEy + c.ob, in.xb, in.xa, in.pa[2], in.ca[2],
+                               dey, u2, dx, h);
       if ((F & kFY) && cb.yf >= 0) {
-        const Face<T>& F = p.face[cb.yf];
-        cpml_apply_loaded<T, C, EXACT, false>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 1, in.pb[2],
-                                              in.cb[2], dex, u1, dy, h);
+        const Face<T>& fc = p.face[cb.yf];
+        cpml_fold<T, C, EXACT>(p.coef, fc.psi[1] + (i * fc.nc + cb.yci) * nzp1 + c.k, cb.yb, cb.ya, in.pb[2], in.cb[2],
+                               dex, u1, dy, h);
       }
       f.Hz[i * sHzEy + c.ob] = h;
     }
@@ -541,7 +566,7 @@ __device__ __forceinline__ void h_band_store(const StepParams<T, C>& p, const HC
 // Planes [a, b) of a column in the band form: every load of a plane is
 // issued before its stores; with BPF the next plane's loads are also in flight.
 template <typename T, class C, bool EXACT, bool BPF, unsigned F = kFAll>
-__device__ __forceinline__ void h_band_range(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int a,
+__device__ __forceinline__ void h_band_range(const StepParams<T, C>& p, const HCol<T>& c, const ColBands<T>& cb, int a,
                                              int b, T& ez_c, T& ey_c) {
   if (a >= b) return;
   HBand<T, C> cur, nxt;
@@ -716,7 +741,7 @@ __device__ __forceinline__ void h_lean_range(const StepParams<T, C>& p, const HC
 // band membership is YZ: the edge planes (an x band may apply) with x added,
 // the x-interior planes [xa, xb) with YZ only, or lean when YZ is empty.
 template <typename T, class C, bool EXACT, int PF, unsigned YZ>
-__device__ __forceinline__ void h_tile_planes(const StepParams<T, C>& p, const HCol<T>& c, const ColBands& cb, int i0,
+__device__ __forceinline__ void h_tile_planes(const StepParams<T, C>& p, const HCol<T>& c, const ColBands<T>& cb, int i0,
                                               int xa, int xb, int i1, T& ez_c, T& ey_c) {
   constexpr bool BPF = BandForm<C>::kPrefetch;
   h_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, i0, xa, ez_c, ey_c);
@@ -767,9 +792,7 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
   const int xa = min(max(i0, lo), i1);
   const int xb = max(xa, min(i1, hi));
   if (BandForm<C>::kUse && p.bands_disjoint != 0) {
-    ColBands cb{};
-    cb.yf = band_face(p.face, 1, j, false, cb.yci);
-    cb.zf = band_face(p.face, 2, k, false, cb.zci);
+    const ColBands<T> cb = col_bands<T, false>(p.face, j, k);
     if (warp_y) {
       if (warp_z)
         h_tile_planes<T, C, EXACT, PF, kFY | kFZ>(p, c, cb, i0, xa, xb, i1, ez_c, ey_c);
@@ -1047,12 +1070,13 @@ struct EBand {
   typename C::Raw r0, r1, r2;
   float kex;            // 1/kappa_e at plane i
   int xf, xci;          // x band of plane i, or -1
+  T xb, xa;             // its profile values
   T pa[3], pb[3];       // Psi of the first / second correcting face of Ex, Ey, Ez
   T ca[3], cb[3];
 };
 
 template <typename T, class C, unsigned F = kFAll>
-__device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
+__device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECol<T>& c, const ColBands<T>& cb, int i,
                                             EBand<T, C>& in) {
   const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
   const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
@@ -1062,6 +1086,7 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
   in.hy_i = c.ez_ok ? (inx ? f.Hy[i * sHyEz + c.oa] : f.Hz[c.oa]) : T(0);
   if (F & kFX) {
     in.xf = band_face(p.face, 0, i, true, in.xci);
+    band_profile<T, true>(p.face, in.xf, in.xci, in.xb, in.xa);
     in.kex = p.coef.invk(0, i);
   } else {
     in.xf = -1;
@@ -1076,16 +1101,16 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     if (c.kz) in.hy_km = f.Hy[i * sHyEz + c.oa - 1];
     in.r0 = p.coef.fetch(3, idx);
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      const int pi = (i * F.nc + cb.yci) * nzp1 + c.k;
-      in.pa[0] = F.psi[3][pi];
-      in.ca[0] = p.coef.cpsi_fetch(F, 3, pi);
+      const Face<T>& fc = p.face[cb.yf];
+      const int pi = (i * fc.nc + cb.yci) * nzp1 + c.k;
+      in.pa[0] = fc.psi[3][pi];
+      in.ca[0] = p.coef.cpsi_fetch(fc, 3, pi);
     }
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      const int pi = (i * nyp1 + c.j) * F.nc + cb.zci;
-      in.pb[0] = F.psi[2][pi];
-      in.cb[0] = p.coef.cpsi_fetch(F, 2, pi);
+      const Face<T>& fc = p.face[cb.zf];
+      const int pi = (i * nyp1 + c.j) * fc.nc + cb.zci;
+      in.pb[0] = fc.psi[2][pi];
+      in.cb[0] = p.coef.cpsi_fetch(fc, 2, pi);
     }
   }
   if (c.ey_ok) {
@@ -1094,16 +1119,16 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     if (c.kz) in.hx_km = f.Hx[i * sHx + c.oa - 1];
     in.r1 = p.coef.fetch(4, idx);
     if ((F & kFX) && in.xf >= 0) {
-      const Face<T>& F = p.face[in.xf];
+      const Face<T>& fc = p.face[in.xf];
       const int pi = in.xci * sHzEy + c.ob;
-      in.pa[1] = F.psi[2][pi];
-      in.ca[1] = p.coef.cpsi_fetch(F, 2, pi);
+      in.pa[1] = fc.psi[2][pi];
+      in.ca[1] = p.coef.cpsi_fetch(fc, 2, pi);
     }
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      const int pi = (i * ny + c.j) * F.nc + cb.zci;
-      in.pb[1] = F.psi[3][pi];
-      in.cb[1] = p.coef.cpsi_fetch(F, 3, pi);
+      const Face<T>& fc = p.face[cb.zf];
+      const int pi = (i * ny + c.j) * fc.nc + cb.zci;
+      in.pb[1] = fc.psi[3][pi];
+      in.cb[1] = p.coef.cpsi_fetch(fc, 3, pi);
     }
   }
   if (c.ez_ok) {
@@ -1112,16 +1137,16 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
     if (c.jy) in.hx_jm = f.Hx[i * sHx + c.oa - nz];
     in.r2 = p.coef.fetch(5, idx);
     if ((F & kFX) && in.xf >= 0) {
-      const Face<T>& F = p.face[in.xf];
+      const Face<T>& fc = p.face[in.xf];
       const int pi = in.xci * sHyEz + c.oa;
-      in.pa[2] = F.psi[3][pi];
-      in.ca[2] = p.coef.cpsi_fetch(F, 3, pi);
+      in.pa[2] = fc.psi[3][pi];
+      in.ca[2] = p.coef.cpsi_fetch(fc, 3, pi);
     }
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      const int pi = (i * F.nc + cb.yci) * nz + c.k;
-      in.pb[2] = F.psi[2][pi];
-      in.cb[2] = p.coef.cpsi_fetch(F, 2, pi);
+      const Face<T>& fc = p.face[cb.yf];
+      const int pi = (i * fc.nc + cb.yci) * nz + c.k;
+      in.pb[2] = fc.psi[2][pi];
+      in.cb[2] = p.coef.cpsi_fetch(fc, 2, pi);
     }
   }
 }
@@ -1129,7 +1154,7 @@ __device__ __forceinline__ void e_band_load(const StepParams<T, C>& p, const ECo
 // e_plane<LEAN=false> on preloaded inputs (bands disjoint): identical
 // arithmetic in the identical order.
 template <typename T, class C, bool EXACT, unsigned F = kFAll>
-__device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i,
+__device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const ECol<T>& c, const ColBands<T>& cb, int i,
                                              int ts, const EBand<T, C>& in, T& hz_p, T& hy_p) {
   const float key = (F & kFY) ? c.key : 1.f, kez = (F & kFZ) ? c.kez : 1.f;
   using A = Ar<T, EXACT>;
@@ -1145,14 +1170,14 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     p.coef.decode_k(3, in.r0, key, kez, c0, c1, c2, u1, u2);
     if (c.jy && c.kz) e = A::lin3(c0, e, c1, dhz, c2, dhy);
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nzp1 + c.k, 3, in.pa[0], in.ca[0],
-                                           dhz, u1, dy, e);
+      const Face<T>& fc = p.face[cb.yf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[3] + (i * fc.nc + cb.yci) * nzp1 + c.k, cb.yb, cb.ya, in.pa[0], in.ca[0],
+                             dhz, u1, dy, e);
     }
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * nyp1 + c.j) * F.nc + cb.zci, 2, in.pb[0], in.cb[0],
-                                           dhy, u2, dz, e);
+      const Face<T>& fc = p.face[cb.zf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[2] + (i * nyp1 + c.j) * fc.nc + cb.zci, cb.zb, cb.za, in.pb[0], in.cb[0],
+                             dhy, u2, dz, e);
     }
     if (c.sx) inject_masked(p.src, c.sx, i, c.j, c.k, ts, e);
     f.Ex[i * sEx + c.ob] = e;
@@ -1164,12 +1189,12 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     p.coef.decode_k(4, in.r1, kez, in.kex, c0, c1, c2, u1, u2);
     if (i >= 1 && c.kz) e = A::lin3(c0, e, c1, dhx, c2, dhz);
     if ((F & kFX) && in.xf >= 0)
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHzEy + c.ob, 2, in.pa[1],
-                                           in.ca[1], dhz, u2, dx, e);
+      cpml_fold<T, C, EXACT>(p.coef, p.face[in.xf].psi[2] + in.xci * sHzEy + c.ob, in.xb, in.xa, in.pa[1], in.ca[1],
+                             dhz, u2, dx, e);
     if ((F & kFZ) && cb.zf >= 0) {
-      const Face<T>& F = p.face[cb.zf];
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.zci, (i * ny + c.j) * F.nc + cb.zci, 3, in.pb[1], in.cb[1],
-                                           dhx, u1, dz, e);
+      const Face<T>& fc = p.face[cb.zf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[3] + (i * ny + c.j) * fc.nc + cb.zci, cb.zb, cb.za, in.pb[1], in.cb[1], dhx,
+                             u1, dz, e);
     }
     if (c.sy) inject_masked(p.src, c.sy, i, c.j, c.k, ts, e);
     f.Ey[i * sHzEy + c.ob] = e;
@@ -1181,12 +1206,12 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     p.coef.decode_k(5, in.r2, in.kex, key, c0, c1, c2, u1, u2);
     if (i >= 1 && c.jy) e = A::lin3(c0, e, c1, dhy, c2, dhx);
     if ((F & kFX) && in.xf >= 0)
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, p.face[in.xf], in.xci, in.xci * sHyEz + c.oa, 3, in.pa[2],
-                                           in.ca[2], dhy, u1, dx, e);
+      cpml_fold<T, C, EXACT>(p.coef, p.face[in.xf].psi[3] + in.xci * sHyEz + c.oa, in.xb, in.xa, in.pa[2], in.ca[2],
+                             dhy, u1, dx, e);
     if ((F & kFY) && cb.yf >= 0) {
-      const Face<T>& F = p.face[cb.yf];
-      cpml_apply_loaded<T, C, EXACT, true>(p.coef, F, cb.yci, (i * F.nc + cb.yci) * nz + c.k, 2, in.pb[2], in.cb[2],
-                                           dhx, u2, dy, e);
+      const Face<T>& fc = p.face[cb.yf];
+      cpml_fold<T, C, EXACT>(p.coef, fc.psi[2] + (i * fc.nc + cb.yci) * nz + c.k, cb.yb, cb.ya, in.pb[2], in.cb[2], dhx,
+                             u2, dy, e);
     }
     if (c.sz) inject_masked(p.src, c.sz, i, c.j, c.k, ts, e);
     f.Ez[i * sHyEz + c.oa] = e;
@@ -1196,7 +1221,7 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
 }
 
 template <typename T, class C, bool EXACT, bool BPF, unsigned F = kFAll>
-__device__ __forceinline__ void e_band_range(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int a,
+__device__ __forceinline__ void e_band_range(const StepParams<T, C>& p, const ECol<T>& c, const ColBands<T>& cb, int a,
                                              int b, int ts, T& hz_p, T& hy_p) {
   if (a >= b) return;
   EBand<T, C> cur, nxt;
@@ -1263,7 +1288,7 @@ __device__ __forceinline__ void e_lean_range(const StepParams<T, C>& p, const EC
 // Planes [i0, i1) of an E column in the band form (see h_tile_planes); the
 // edge ranges also hold the boundary planes i = 0 and i = nx.
 template <typename T, class C, bool EXACT, int PF, unsigned YZ>
-__device__ __forceinline__ void e_tile_planes(const StepParams<T, C>& p, const ECol<T>& c, const ColBands& cb, int i0,
+__device__ __forceinline__ void e_tile_planes(const StepParams<T, C>& p, const ECol<T>& c, const ColBands<T>& cb, int i0,
                                               int xa, int xb, int i1, int ts, T& hz_p, T& hy_p) {
   constexpr bool BPF = BandForm<C>::kPrefetch;
   e_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, i0, xa, ts, hz_p, hy_p);
@@ -1316,9 +1341,7 @@ __device__ __forceinline__ void step_e_tile(const StepParams<T, C>& p, int bx, i
   const int xa = min(max(i0, max(lo, 1)), i1);
   const int xb = max(xa, min(i1, min(hi, nx)));
   if (BandForm<C>::kUse && p.bands_disjoint != 0) {
-    ColBands cb{};
-    cb.yf = band_face(p.face, 1, j, true, cb.yci);
-    cb.zf = band_face(p.face, 2, k, true, cb.zci);
+    const ColBands<T> cb = col_bands<T, true>(p.face, j, k);
     if (warp_src) {  // source columns: the general form on every plane
       e_band_range<T, C, EXACT, BandForm<C>::kPrefetch, kFAll>(p, c, cb, i0, i1, ts, hz_p, hy_p);
     } else if (warp_y) {
