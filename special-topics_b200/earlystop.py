@@ -294,25 +294,29 @@ def extend(V, I, mode: Mode, n_stop: int, n_total: int, dt: float):
 # Transients from the batched solver
 # ---------------------------------------------------------------------------
 def _variant_problem(args):
-    seed, steps = args
+    seed, steps, per_cell = (*args, False) if len(args) == 2 else args
     from .scenario import build_problem_from_scenario
     from .workloads import ifa_variant
-    return build_problem_from_scenario(ifa_variant(seed, steps=steps), steps, per_cell=False)
+    return build_problem_from_scenario(ifa_variant(seed, steps=steps), steps, per_cell=per_cell)
 
 
-def variant_problems(seeds, steps: int, pool=None) -> list:
+def variant_problems(seeds, steps: int, pool=None, per_cell: bool = False) -> list:
     """Problems of the inverted-F variant family (workloads.ifa_variant).
-    A process pool must make this package importable in its workers first
-    (an initializer that loads it), or the workers cannot run the jobs."""
-    jobs = [(int(s), steps) for s in seeds]
+    per_cell=False (FP32 material tables) carries the material grid only;
+    per_cell=True adds the 18 FP64 coefficient arrays the FP64 engine needs
+    (about 170 MB per variant, so build those a group at a time).  A process
+    pool must make this package importable in its workers first (an
+    initializer that loads it), or the workers cannot run the jobs."""
+    jobs = [(int(s), steps, per_cell) for s in seeds]
     return pool.map(_variant_problem, jobs) if pool is not None else [_variant_problem(j) for j in jobs]
 
 
 def run_variants(problems, steps: int, precision: str = "f32-table", group: int = 128, device: int = 0,
-                 tiling: dict | None = None):
+                 tiling: dict | None = None, progress=None):
     """Runs the problems `steps` steps in batches of `group` (launch shape
     `tiling`, as Batch.tiling() returns it) and returns the port traces V, I
-    (len(problems) x steps, FP64) and the device seconds of the stepping."""
+    (len(problems) x steps, FP64) and the device seconds of the stepping.
+    `progress(msg)`, if given, is called after every batch."""
     from .backend import Batch, Engine
     V = np.zeros((len(problems), steps))
     I = np.zeros((len(problems), steps))
@@ -330,6 +334,8 @@ def run_variants(problems, steps: int, precision: str = "f32-table", group: int 
         finally:
             for e in engs:
                 e.close()
+        if progress:
+            progress(f"{g0 + len(engs)} of {len(problems)} runs, {device_s:.1f} device s")
     return V, I, device_s
 
 

@@ -60,14 +60,22 @@ def _label(args):
 
 
 LABEL_END = 4500
+_T0 = time.perf_counter()
+
+
+def log(msg: str) -> None:
+    print(f"[{time.perf_counter() - _T0:8.1f} s] {msg}", flush=True)
 
 
 def build_set(ES, pool, seeds, steps, policy, tiling):
     probs = ES.variant_problems(seeds, steps, pool)
-    V, I, dev_s = ES.run_variants(probs, LABEL_END, "f32-table", tiling=tiling)
+    log(f"{len(probs)} training problems built")
+    V, I, dev_s = ES.run_variants(probs, LABEL_END, "f32-table", tiling=tiling, progress=log)
+    log(f"training transients done ({dev_s:.1f} device s)")
     dts = [p.grid.dt for p in probs]
     # labels from the steps before the FP32 runs' late-time growth sets in
     labels = pool.map(_label, [(V[q], I[q], policy.n_in, LABEL_END, dts[q]) for q in range(len(seeds))])
+    log(f"{sum(t is not None for t in labels)} labels")
     x, y, keep = [], [], []
     for q, t in enumerate(labels):
         if t is None:
@@ -79,13 +87,17 @@ def build_set(ES, pool, seeds, steps, policy, tiling):
     return np.array(x, np.float32), np.array(y, np.float32), keep, dev_s
 
 
-def plain_reference(ES, probs, policy, tiling, group=128):
-    """S11 of plain FP64 batched runs of the full step count, and their wall time."""
+def plain_reference(ES, pool, seeds, policy, tiling, group=64):
+    """S11 of plain FP64 batched runs of the full step count, and their wall
+    time (problem construction excluded).  The FP64 problems carry per-cell
+    coefficient arrays, so they are built one group at a time."""
     from special_topics_b200.backend import Batch, Engine
     freqs = ES.S11_FREQS
+    seeds = list(seeds)
     ref, t_plain = [], 0.0
-    for g0 in range(0, len(probs), group):
-        engs = [Engine(p, "f64") for p in probs[g0:g0 + group]]
+    for g0 in range(0, len(seeds), group):
+        probs = ES.variant_problems(seeds[g0:g0 + group], policy.n_total, pool, per_cell=True)
+        engs = [Engine(p, "f64") for p in probs]
         try:
             t0 = time.perf_counter()
             with Batch(engs) as b:
@@ -98,6 +110,8 @@ def plain_reference(ES, probs, policy, tiling, group=128):
         finally:
             for e in engs:
                 e.close()
+        del probs, engs
+        log(f"plain FP64 reference: {min(g0 + group, len(seeds))} of {len(seeds)} runs")
     return np.array(ref), t_plain
 
 
@@ -115,6 +129,7 @@ def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128):
                 res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use_net)
                 s11 = [ES.s11_db(r["V"], r["I"], e.problem.grid.dt, freqs) for r, e in zip(res, engs)]
                 t += time.perf_counter() - t0
+                log(f"{name}: {g0 + len(engs)} of {len(probs)} runs")
             finally:
                 for e in engs:
                     e.close()
@@ -165,6 +180,9 @@ def main():
     ap.add_argument("--cache", default=None, help="npz of a previous run's training set and test reference")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    # one BLAS thread per pool worker (inherited by the spawned processes)
+    for v in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
     # workers register the package under its import name before any task arrives
     pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1), initializer=_package)
     _package()
@@ -175,6 +193,7 @@ def main():
     t0 = time.perf_counter()
     test_seeds = range(10000, 10000 + args.test)
     test_probs = ES.variant_problems(test_seeds, policy.n_total, pool)
+    log(f"{len(test_probs)} test problems built")
     if args.cache and os.path.exists(args.cache):
         z = np.load(args.cache)
         x, y, ref, t_plain = z["x"], z["y"], z["ref"], float(z["t_plain"])
@@ -183,7 +202,8 @@ def main():
         x, y, keep, dev_s = build_set(ES, pool, range(1000, 1000 + args.train), policy.n_total, policy, tiling)
         metrics["train_set"] = {"runs": args.train, "labelled": len(keep), "solver_device_s": dev_s,
                                 "wall_s": time.perf_counter() - t0}
-        ref, t_plain = plain_reference(ES, test_probs, policy, tiling)
+        np.savez(os.path.join(args.out, "es_train_set.npz"), x=x, y=y)
+        ref, t_plain = plain_reference(ES, pool, test_seeds, policy, tiling)
         np.savez(os.path.join(args.out, "es_data.npz"), x=x, y=y, ref=ref, t_plain=t_plain)
     # target scaling: each output standardised over the training set
     mu, sd = y.mean(axis=0), y.std(axis=0) + 1e-6
@@ -208,6 +228,9 @@ def main():
                                                                       axis=0).tolist()}
     net.out_mu, net.out_sd = mu.astype(np.float32), sd.astype(np.float32)
     net.save(os.path.join(args.out, "es_weights.npz"))
+    log(f"trained: {metrics['training']}")
+    with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
+        json.dump(metrics, f, indent=1)
     metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling)
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
