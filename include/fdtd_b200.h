@@ -200,9 +200,10 @@ typedef struct fdtd_batch fdtd_batch;
 
 /* Groups `count` handles of one device and one precision.  The batch owns no
  * member: members stay valid handles (readbacks, fdtd_status, their own runs)
- * and must outlive the batch.  Each step of fdtd_batch_run is four launches for
- * the whole batch: H over a tile list spanning every member, the mid-step
- * kernel, E over the tile list, and the far-field/port epilogue. */
+ * and must outlive the batch.  By default each step of fdtd_batch_run is four
+ * launches for the whole batch: H over a tile list spanning every member, the
+ * mid-step kernel, E over the tile list, and the far-field/port epilogue
+ * (fdtd_batch_set_streams selects the member-kernel mode instead). */
 int fdtd_batch_create(fdtd_ctx* const* members, int count, fdtd_batch** out);
 void fdtd_batch_free(fdtd_batch* batch);
 int fdtd_batch_size(const fdtd_batch* batch);
@@ -214,12 +215,22 @@ int fdtd_batch_size(const fdtd_batch* batch);
 int fdtd_batch_set_tiling(fdtd_batch* batch, int x_planes_per_thread, int block_rows, int prefetch, int group);
 int fdtd_batch_get_tiling(const fdtd_batch* batch, int* x_planes_per_thread, int* block_rows, int* prefetch,
                           int* group);
+/* Member-kernel mode: streams = S > 0 runs each member's own step kernels
+ * (those of fdtd_ctx_run, with the batch's launch shape), the members spread
+ * over S worker streams inside one CUDA graph, all steps of a graph for one
+ * member before the next member of its stream (so a member's arrays stay in L2
+ * from one step to the next).  streams = 0 (default) is the tile-list mode.
+ * Results are identical in both modes.  S <= 32. */
+int fdtd_batch_set_streams(fdtd_batch* batch, int streams);
+int fdtd_batch_get_streams(const fdtd_batch* batch, int* streams);
 /* Runs `count` steps of every member.  All members must be at the same step and
  * have `count` steps left.  Returns FDTD_ERR_NONFINITE naming the first member
  * whose watchdog fired. */
 int fdtd_batch_run(fdtd_batch* batch, int count);
 int fdtd_batch_run_timed(fdtd_batch* batch, int count, float* ms);
-/* Per-kernel mean durations (ms) of the batch's H, mid-step, E and epilogue launches. */
+/* Per-kernel mean durations (ms) of the batch's H, mid-step, E and epilogue
+ * launches per step (member-kernel mode: each member timed alone, summed over
+ * the members). */
 int fdtd_batch_profile_kernels(fdtd_batch* batch, int count, double* avg_ms);
 
 /* Whole probe traces, FP64, one value per step (first `n` steps). kind 0 = voltage, 1 = current. */

@@ -85,6 +85,10 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
 
 BATCH_CHUNKS = (2, 4, 8, 16, 32)
 BATCH_GROUPS = (0, 1, 2, 4, 8, 16)
+# member-kernel mode: worker stream counts and member launch shapes tried
+BATCH_STREAMS = (2, 3, 4, 6, 8, 16)
+MEMBER_SHAPES = ((32, 4, 1), (16, 4, 1), (32, 8, 1), (64, 4, 1))
+MEMBER_STEPS = 64   # member-kernel trials time whole graphs of this many steps
 
 
 def batch_key(batch) -> str:
@@ -97,30 +101,36 @@ def batch_key(batch) -> str:
 
 
 def batch_steps_needed(steps_per_candidate: int, precision: str = "f32-table") -> int:
-    return 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(prefetch_depths(precision))
-                                      + len(BATCH_GROUPS))
+    tile_mode = 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(prefetch_depths(precision))
+                                           + len(BATCH_GROUPS))
+    member_mode = 2 * MEMBER_STEPS * (len(BATCH_STREAMS) + len(MEMBER_SHAPES))
+    return tile_mode + member_mode
 
 
 def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> dict:
-    """Tunes a batch's shared launch shape on the batch itself (every shape
-    computes the same values, so tuning only advances the members by
-    batch_steps_needed(steps_per_candidate) steps).  First x planes per thread,
-    block rows and prefetch depth with one block per tile, then the tile group
-    of the persistent grid at that shape.  Sets and returns the fastest."""
+    """Tunes a batch's launch shape on the batch itself (every shape computes
+    the same values, so tuning only advances the members by
+    batch_steps_needed(steps_per_candidate) steps).  Tile-list mode: x planes
+    per thread, block rows and prefetch depth with one block per tile, then
+    the tile group of the persistent grid.  Member-kernel mode: the worker
+    stream count at the first member shape, then the member shapes at the best
+    count (whole graphs of MEMBER_STEPS steps, since a member-mode step is
+    many launches).  Sets and returns the fastest."""
     key = batch_key(batch)
     cache = _load()
     if use_cache and key in cache:
         r = cache[key]
-        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"])
+        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"], r.get("streams", 0))
         return r
     max_x = max(e.problem.grid.nx for e in batch.engines) + 1
     table = []
 
-    def trial(chunk, rows, pf, group):
-        batch.set_tiling(chunk, rows, pf, group)
-        batch.run_timed(steps_per_candidate)              # capture and warm the graph
-        ms = batch.run_timed(steps_per_candidate) / steps_per_candidate
-        table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "ms_per_step": ms})
+    def trial(chunk, rows, pf, group, streams=0, steps=steps_per_candidate):
+        batch.set_tiling(chunk, rows, pf, group, streams)
+        batch.run_timed(steps)              # capture and warm the graph
+        ms = batch.run_timed(steps) / steps
+        table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams,
+                      "ms_per_step": ms})
 
     for chunk in BATCH_CHUNKS:
         for rows in ROWS:
@@ -129,9 +139,15 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
     best = min(table, key=lambda r: r["ms_per_step"])
     for group in BATCH_GROUPS[1:]:
         trial(best["chunk"], best["rows"], best["prefetch"], group)
+    ch, rw, pf = MEMBER_SHAPES[0]
+    for streams in BATCH_STREAMS:
+        trial(min(ch, max_x), rw, pf, 0, streams, MEMBER_STEPS)
+    s_best = min((r for r in table if r["streams"] > 0), key=lambda r: r["ms_per_step"])["streams"]
+    for ch, rw, pf in MEMBER_SHAPES[1:]:
+        trial(min(ch, max_x), rw, pf, 0, s_best, MEMBER_STEPS)
     best = min(table, key=lambda r: r["ms_per_step"])
     out = dict(best, table=table)
-    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"])
+    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"], best["streams"])
     cache[key] = out
     os.makedirs(os.path.dirname(CACHE), exist_ok=True)
     with open(CACHE, "w") as f:

@@ -241,11 +241,14 @@ class Engine:
 
 
 class Batch:
-    """Engines of one precision on one device advanced together: every step is
-    four launches for the whole batch (fdtd_batch_* in include/fdtd_b200.h).
-    The engines stay usable for readback and must outlive the batch."""
+    """Engines of one precision on one device advanced together
+    (fdtd_batch_* in include/fdtd_b200.h).  streams = 0: every step is four
+    launches for the whole batch over a tile list; streams = S > 0: each
+    member's own step kernels on S worker streams in one graph.  The engines
+    stay usable for readback and must outlive the batch."""
 
-    def __init__(self, engines: list, chunk: int = 8, rows: int = 4, prefetch: int = 1, group: int = 0):
+    def __init__(self, engines: list, chunk: int = 8, rows: int = 4, prefetch: int = 1, group: int = 0,
+                 streams: int = 0):
         if not engines:
             raise ValueError("a batch needs at least one engine")
         self.engines = list(engines)
@@ -253,15 +256,25 @@ class Batch:
         h = C.c_void_p()
         N.check(N.lib().fdtd_batch_create(arr, len(self.engines), C.byref(h)))
         self._h = h
-        self.set_tiling(chunk, rows, prefetch, group)
+        self.set_tiling(chunk, rows, prefetch, group, streams)
 
-    def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0) -> None:
+    def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0, streams: int | None = None) -> None:
+        """Launch shape (see fdtd_batch_set_tiling) and, when given, the
+        member-kernel worker stream count (fdtd_batch_set_streams)."""
         N.check(N.lib().fdtd_batch_set_tiling(self._h, int(chunk), int(rows), int(prefetch), int(group)))
+        if streams is not None:
+            N.check(N.lib().fdtd_batch_set_streams(self._h, int(streams)))
+
+    def set_shape(self, shape: dict) -> None:
+        """set_tiling from a dict as tiling() returns it ("streams" optional)."""
+        self.set_tiling(shape["chunk"], shape["rows"], shape.get("prefetch", 1), shape.get("group", 0),
+                        shape.get("streams", 0))
 
     def tiling(self) -> dict:
-        v = [C.c_int() for _ in range(4)]
-        N.check(N.lib().fdtd_batch_get_tiling(self._h, *[C.byref(x) for x in v]))
-        return dict(zip(("chunk", "rows", "prefetch", "group"), [x.value for x in v]))
+        v = [C.c_int() for _ in range(5)]
+        N.check(N.lib().fdtd_batch_get_tiling(self._h, *[C.byref(x) for x in v[:4]]))
+        N.check(N.lib().fdtd_batch_get_streams(self._h, C.byref(v[4])))
+        return dict(zip(("chunk", "rows", "prefetch", "group", "streams"), [x.value for x in v]))
 
     @property
     def cells(self) -> int:

@@ -406,10 +406,11 @@ struct KernelTimer {
   double ms[4] = {0, 0, 0, 0};
 };
 
-// Enqueue `count` steps on the handle's stream (with `tm`, one step at a time,
-// timing each kernel).
+// Enqueue `count` steps on stream `st` (default: the handle's stream; with
+// `tm`, one step at a time, timing each kernel).
 template <typename T, class C, bool EXACT>
-int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullptr) {
+int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullptr, cudaStream_t st = nullptr) {
+  if (!st) st = c->stream;
   StepParams<T, C> p = step_params<T, C>(c, coef);
   Probes pr = dev_probes(c);
   FarField ff = dev_ff(c);
@@ -429,17 +430,17 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   if (!rc) rc = stage_smem(ke, c->prefetch, 32 * c->block_rows, &smem);
   if (rc) return rc;
   for (int s = 0; s < count; s++) {
-    if (tm) CK(cudaEventRecord(tm->ev[0], c->stream));
-    kh<<<grd, blk, smem, c->stream>>>(p);
-    if (tm) CK(cudaEventRecord(tm->ev[1], c->stream));
-    k_step_mid<T, C, EXACT><<<mid_blocks, 256, 0, c->stream>>>(p, pr);
-    if (tm) CK(cudaEventRecord(tm->ev[2], c->stream));
-    ke<<<grd, blk, smem, c->stream>>>(p);
-    if (tm) CK(cudaEventRecord(tm->ev[3], c->stream));
-    if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, c->stream>>>(p.f, p.g, ff, pr, c->d_ts);
-    if (c->dft_block > 0) k_dft_flush<<<flush_blocks, 256, 0, c->stream>>>(ff, c->d_ts, -1);
+    if (tm) CK(cudaEventRecord(tm->ev[0], st));
+    kh<<<grd, blk, smem, st>>>(p);
+    if (tm) CK(cudaEventRecord(tm->ev[1], st));
+    k_step_mid<T, C, EXACT><<<mid_blocks, 256, 0, st>>>(p, pr);
+    if (tm) CK(cudaEventRecord(tm->ev[2], st));
+    ke<<<grd, blk, smem, st>>>(p);
+    if (tm) CK(cudaEventRecord(tm->ev[3], st));
+    if (epi_blocks) k_epilogue<T><<<epi_blocks, 256, 0, st>>>(p.f, p.g, ff, pr, c->d_ts);
+    if (c->dft_block > 0) k_dft_flush<<<flush_blocks, 256, 0, st>>>(ff, c->d_ts, -1);
     if (tm) {
-      CK(cudaEventRecord(tm->ev[4], c->stream));
+      CK(cudaEventRecord(tm->ev[4], st));
       CK(cudaEventSynchronize(tm->ev[4]));
       for (int q = 0; q < 4; q++) {
         float ms = 0;
@@ -509,13 +510,30 @@ int prepare_table(fdtd_ctx* c, TableCoef* out) {
   return FDTD_OK;
 }
 
-int enqueue(fdtd_ctx* c, int count, KernelTimer* tm = nullptr) {
-  if (c->prec == FDTD_PREC_F64) return enqueue_steps<double, ArrayCoef<double>, true>(c, array_coef<double>(c), count, tm);
-  if (c->prec == FDTD_PREC_F32) return enqueue_steps<float, ArrayCoef<float>, true>(c, array_coef<float>(c), count, tm);
-  return enqueue_steps<float, TableCoef, false>(c, c->tcoef, count, tm);
+int enqueue(fdtd_ctx* c, int count, KernelTimer* tm = nullptr, cudaStream_t st = nullptr) {
+  if (c->prec == FDTD_PREC_F64)
+    return enqueue_steps<double, ArrayCoef<double>, true>(c, array_coef<double>(c), count, tm, st);
+  if (c->prec == FDTD_PREC_F32)
+    return enqueue_steps<float, ArrayCoef<float>, true>(c, array_coef<float>(c), count, tm, st);
+  return enqueue_steps<float, TableCoef, false>(c, c->tcoef, count, tm, st);
+}
+
+// End of a run that reached step `upto` with the time-blocked DFT: accumulate
+// what the run left buffered (the open block) and mark it done.
+int close_dft_block(fdtd_ctx* c, int upto, cudaStream_t st) {
+  if (c->dft_block <= 0) return FDTD_OK;
+  if (upto % c->dft_block != 0) {
+    const long long n = (c->ffsz[0] + c->ffsz[1] + c->ffsz[2]) * (long long)c->nFreq;
+    k_dft_flush<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dev_ff(c), c->d_ts, upto);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(c->d_dft_done, &upto, sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));  // `upto` is read from this frame
+  return FDTD_OK;
 }
 
 constexpr int kGraphSteps = 64;
+constexpr int kMaxBatchStreams = 32;
 
 int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* tm = nullptr) {
   if (count < 0) return fail(FDTD_ERR_BADARG, "negative step count %d", count);
@@ -574,15 +592,9 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
   }
-  if (c->dft_block > 0 && count > 0) {
-    // close the open block: accumulate what the run left buffered
-    const int upto = c->ts + count;
-    if (upto % c->dft_block != 0) {
-      const long long n = (c->ffsz[0] + c->ffsz[1] + c->ffsz[2]) * (long long)c->nFreq;
-      k_dft_flush<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(dev_ff(c), c->d_ts, upto);
-      CK(cudaGetLastError());
-    }
-    CK(cudaMemcpyAsync(c->d_dft_done, &upto, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (count > 0) {
+    rc = close_dft_block(c, c->ts + count, c->stream);
+    if (rc) return rc;
   }
   CK(cudaStreamSynchronize(c->stream));
   c->ts += count;
@@ -1540,6 +1552,12 @@ struct fdtd_batch {
   BatchBlock* d_flush = nullptr;
   int grid_h = 0, grid_e = 0;  // persistent grid sizes
   cudaGraphExec_t graph = nullptr;
+  // member-kernel mode (streams > 0): each member's own step kernels, members
+  // spread over `streams` worker streams joined to `stream`
+  int streams = 0;
+  std::vector<cudaStream_t> ws;
+  std::vector<cudaEvent_t> wev;
+  cudaEvent_t fork_ev = nullptr;
 };
 
 namespace {
@@ -1727,6 +1745,118 @@ int batch_enqueue_any(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
   return batch_enqueue<float, TableCoef, false>(b, count, tm);
 }
 
+// Member-kernel mode.  Sets a member's launch shape to the batch's for the
+// duration of a scope (its own shape comes back afterwards).
+struct MemberShape {
+  fdtd_ctx* c;
+  int ichunk, rows, pf;
+  MemberShape(fdtd_ctx* m, const fdtd_batch* b) : c(m), ichunk(m->ichunk), rows(m->block_rows), pf(m->prefetch) {
+    m->ichunk = b->ichunk;
+    m->block_rows = b->block_rows;
+    m->prefetch = b->prefetch;
+  }
+  ~MemberShape() {
+    c->ichunk = ichunk;
+    c->block_rows = rows;
+    c->prefetch = pf;
+  }
+};
+
+int batch_worker_streams(fdtd_batch* b) {
+  while ((int)b->ws.size() < b->streams) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->ws.push_back(st);
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->wev.push_back(ev);
+  }
+  if (!b->fork_ev) CK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+  return FDTD_OK;
+}
+
+// `count` steps of every member, member-major: worker stream s steps members
+// s, s + S, s + 2S, ... one after another, all `count` steps of one member
+// before the next, so a member's arrays are still in L2 at its next step.
+// The worker streams fork from and join back into the batch's stream (also
+// under stream capture), and are joined even when an enqueue fails.
+int batch_member_enqueue(fdtd_batch* b, int count) {
+  const int S = b->streams;
+  CK(cudaEventRecord(b->fork_ev, b->stream));
+  for (int q = 0; q < S; q++) CK(cudaStreamWaitEvent(b->ws[q], b->fork_ev, 0));
+  int rc = FDTD_OK;
+  for (size_t q = 0; q < b->m.size() && !rc; q++) {
+    MemberShape shape(b->m[q], b);
+    rc = enqueue(b->m[q], count, nullptr, b->ws[q % S]);
+  }
+  for (int q = 0; q < S; q++) {
+    CK(cudaEventRecord(b->wev[q], b->ws[q]));
+    CK(cudaStreamWaitEvent(b->stream, b->wev[q], 0));
+  }
+  return rc;
+}
+
+int batch_run_members(fdtd_batch* b, int count, float* elapsed_ms, KernelTimer* tm) {
+  const int ts = b->m[0]->ts;
+  int rc = batch_worker_streams(b);
+  if (rc) return rc;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (elapsed_ms) {
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, b->stream));
+  }
+  int left = count;
+  if (tm) {
+    // one member at a time on the batch's stream: per-kernel times summed over members
+    for (size_t q = 0; q < b->m.size() && !rc; q++) {
+      MemberShape shape(b->m[q], b);
+      rc = enqueue(b->m[q], left, tm, b->stream);
+    }
+    if (rc) return rc;
+    left = 0;
+  }
+  while (left >= kGraphSteps) {
+    if (!b->graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int erc = batch_member_enqueue(b, kGraphSteps);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      if (erc) return erc;
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    CK(cudaGraphLaunch(b->graph, b->stream));
+    left -= kGraphSteps;
+  }
+  if (left > 0) {
+    rc = batch_member_enqueue(b, left);
+    if (rc) return rc;
+  }
+  if (elapsed_ms) {
+    CK(cudaEventRecord(ev1, b->stream));
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  for (fdtd_ctx* c : b->m) {
+    rc = count > 0 ? close_dft_block(c, ts + count, b->stream) : FDTD_OK;
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  for (fdtd_ctx* c : b->m) c->ts += count;
+  for (size_t q = 0; q < b->m.size(); q++) {
+    int st[2];
+    CK(cudaMemcpyAsync(st, b->m[q]->d_status, sizeof(st), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    if (st[0] != 0) return fail(FDTD_ERR_NONFINITE, "batch member %zu: non-finite port sample at step %d", q, st[1]);
+  }
+  return FDTD_OK;
+}
+
 int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer* tm = nullptr) {
   if (count < 0) return fail(FDTD_ERR_BADARG, "negative step count %d", count);
   const int ts = b->m[0]->ts;
@@ -1745,6 +1875,7 @@ int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer
     }
   }
   CK(cudaSetDevice(b->device));
+  if (b->streams > 0) return batch_run_members(b, count, elapsed_ms, tm);
   int rc = batch_prepare_any(b);
   if (rc) return rc;
   const int ctl_ts = ts - 1;
@@ -1851,6 +1982,12 @@ void fdtd_batch_free(fdtd_batch* b) {
   cudaFree(b->d_epi);
   cudaFree(b->d_flush);
   cudaFree(b->d_ctl);
+  for (cudaStream_t st : b->ws) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (cudaEvent_t ev : b->wev) cudaEventDestroy(ev);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -1882,6 +2019,21 @@ int fdtd_batch_get_tiling(const fdtd_batch* b, int* x_planes_per_thread, int* bl
   *block_rows = b->block_rows;
   *prefetch = b->prefetch;
   *group = b->group;
+  return FDTD_OK;
+}
+
+int fdtd_batch_set_streams(fdtd_batch* b, int streams) {
+  if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
+  if (streams < 0 || streams > kMaxBatchStreams)
+    return fail(FDTD_ERR_BADARG, "worker streams %d outside 0..%d", streams, kMaxBatchStreams);
+  if (streams != b->streams) batch_drop_graph(b);
+  b->streams = streams;
+  return FDTD_OK;
+}
+
+int fdtd_batch_get_streams(const fdtd_batch* b, int* streams) {
+  if (!b || !streams) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *streams = b->streams;
   return FDTD_OK;
 }
 

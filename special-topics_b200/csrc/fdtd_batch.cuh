@@ -36,25 +36,41 @@ struct BatchCtl {
   int next[2];     // tile counters of the persistent H (0) and E (1) launches
 };
 
+// Copies a parameter block (global) into shared memory with 8-byte words.
+template <class P>
+__device__ __forceinline__ void load_block_params(P* dst, const P* src) {
+  static_assert(sizeof(P) % 8 == 0, "parameter block must be 8-byte sized");
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int w = tid; w < (int)(sizeof(P) / 8); w += nt) d[w] = __ldg(s + w);
+}
+
 // H (ELECTRIC=false) or E (true) update over the batch's tiles.  PERSIST: a
 // persistent grid whose blocks claim `group` consecutive tiles at a time;
-// otherwise one block per tile.
+// otherwise one block per tile.  A block copies its member's parameter block
+// into shared memory: reading it in place from global memory costs more (the
+// loads are repeated after every field store, which may alias them, and what
+// the compiler keeps in registers spills).
 template <typename T, class C, bool EXACT, int PF, bool ELECTRIC, bool PERSIST>
 __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value)
     k_batch_half(const Instance<T, C>* __restrict__ inst, const BatchTile* __restrict__ tiles, int ntiles,
                  BatchCtl* ctl, int group) {
-  // The parameter blocks are read in place: `inst` is const and restrict, so
-  // the field stores cannot alias them and their loads stay hoisted.
+  __shared__ __align__(16) unsigned char raw[sizeof(StepParams<T, C>)];
   __shared__ int s_claim;
+  StepParams<T, C>* sp = reinterpret_cast<StepParams<T, C>*>(raw);
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
   if (!ELECTRIC && blockIdx.x == 0 && lead) ctl->ts += 1;  // first kernel of a step advances the counter
   if constexpr (!PERSIST) {
     const BatchTile t = tiles[blockIdx.x];
+    load_block_params(sp, &inst[t.inst].sp);
+    __syncthreads();
     if (ELECTRIC)
-      step_e_tile<T, C, EXACT, PF>(inst[t.inst].sp, t.bx, t.by, t.bz);
+      step_e_tile<T, C, EXACT, PF>(*sp, t.bx, t.by, t.bz);
     else
-      step_h_tile<T, C, EXACT, PF>(inst[t.inst].sp, t.bx, t.by, t.bz);
+      step_h_tile<T, C, EXACT, PF>(*sp, t.bx, t.by, t.bz);
   } else {
+    int cur = -1;
     for (;;) {
       if (lead) s_claim = atomicAdd(&ctl->next[ELECTRIC ? 1 : 0], group);
       __syncthreads();
@@ -63,10 +79,16 @@ __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value)
       const int last = min(first + group, ntiles);
       for (int q = first; q < last; q++) {
         const BatchTile t = tiles[q];
+        if (t.inst != cur) {
+          __syncthreads();  // every thread is done with the previous block
+          load_block_params(sp, &inst[t.inst].sp);
+          cur = t.inst;
+          __syncthreads();
+        }
         if (ELECTRIC)
-          step_e_tile<T, C, EXACT, PF>(inst[t.inst].sp, t.bx, t.by, t.bz);
+          step_e_tile<T, C, EXACT, PF>(*sp, t.bx, t.by, t.bz);
         else
-          step_h_tile<T, C, EXACT, PF>(inst[t.inst].sp, t.bx, t.by, t.bz);
+          step_h_tile<T, C, EXACT, PF>(*sp, t.bx, t.by, t.bz);
       }
       __syncthreads();  // s_claim is rewritten by the next claim
     }

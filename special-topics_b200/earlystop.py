@@ -30,6 +30,7 @@ from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
+from threadpoolctl import threadpool_limits
 
 from . import _native as N
 
@@ -326,7 +327,7 @@ def run_variants(problems, steps: int, precision: str = "f32-table", group: int 
         try:
             with Batch(engs) as b:
                 if tiling:
-                    b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+                    b.set_shape(tiling)
                 device_s += b.run_timed(steps) / 1e3
             for q, e in enumerate(engs):
                 V[g0 + q] = e.voltages(steps)[0]
@@ -463,7 +464,7 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
     for cp in policy.checkpoints:
         with Batch([engines[q] for q in active]) as b:
             if tiling:
-                b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+                b.set_shape(tiling)
             b.run(cp - b.step)
         if use_network and net is not None and net_poles[active[0]] is None:
             sub = [engines[q] for q in active]
@@ -480,8 +481,10 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
             return best_tail(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
                              net_poles[q] if use_network else None)
 
-        # the fits are LAPACK-bound and release the GIL: one thread per host core
-        with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        # the fits are LAPACK-bound and release the GIL: one thread per host
+        # core, each with a single BLAS thread (16 fits each spreading over
+        # every core oversubscribe the host many times over)
+        with threadpool_limits(limits=1), ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
             fits = list(ex.map(fit_one, range(len(active))))
         for k, q in enumerate(active):
             got = fits[k]

@@ -102,7 +102,7 @@ def plain_reference(ES, pool, seeds, policy, tiling, group=64):
             t0 = time.perf_counter()
             with Batch(engs) as b:
                 if tiling:
-                    b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+                    b.set_shape(tiling)
                 b.run(policy.n_total)
             for e in engs:
                 ref.append(ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs))
@@ -115,7 +115,7 @@ def plain_reference(ES, pool, seeds, policy, tiling, group=64):
     return np.array(ref), t_plain
 
 
-def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128):
+def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out=None):
     """Plain FP64 reference vs the early-stopped FP32 runs (with and without the network)."""
     from special_topics_b200.backend import Batch, Engine
     freqs = ES.S11_FREQS
@@ -143,22 +143,30 @@ def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128):
                      "max_err_dB_p90": float(np.percentile(errs, 90)), "max_err_dB_worst": float(errs.max()),
                      "stops": {str(c): int(np.sum(np.array(stops) == c)) for c in sorted(set(stops))},
                      "winners": {w: winners.count(w) for w in set(winners)}}
-    # plain FP32 runs of the full step count, for context (no early stop)
+    # plain FP32 runs of the full step count, for context (no early stop); their
+    # traces (saved to traces_out) let other stop rules be replayed offline
     errs, t = [], 0.0
+    V32, I32, dts = [], [], []
     for g0 in range(0, len(probs), group):
         engs = [Engine(p, "f32-table") for p in probs[g0:g0 + group]]
         try:
             t0 = time.perf_counter()
             with Batch(engs) as b:
                 if tiling:
-                    b.set_tiling(tiling["chunk"], tiling["rows"], tiling["prefetch"], tiling["group"])
+                    b.set_shape(tiling)
                 b.run(policy.n_total)
             s11 = [ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs) for e in engs]
             t += time.perf_counter() - t0
+            for e in engs:
+                V32.append(e.voltages()[0])
+                I32.append(e.currents()[0])
+                dts.append(e.problem.grid.dt)
         finally:
             for e in engs:
                 e.close()
         errs += [float(np.abs(s11[q] - ref[g0 + q]).max()) for q in range(len(s11))]
+    if traces_out:
+        np.savez(traces_out, V=np.array(V32), I=np.array(I32), dt=np.array(dts), ref=ref)
     errs = np.array(errs)
     out["plain_f32"] = {"time_s": t, "within_0p1_dB": float(np.mean(errs <= 0.1)),
                         "max_err_dB_median": float(np.median(errs)), "max_err_dB_worst": float(errs.max())}
@@ -178,6 +186,8 @@ def main():
     ap.add_argument("--max-resid", type=float, default=1e-4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cache", default=None, help="npz of a previous run's training set and test reference")
+    ap.add_argument("--shape", default="16,4,1,0,0",
+                    help="batch launch shape chunk,rows,prefetch,group,streams (backend.Batch.set_tiling)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     # one BLAS thread per pool worker (inherited by the spawned processes)
@@ -188,7 +198,7 @@ def main():
     _package()
     from special_topics_b200 import earlystop as ES
     policy = ES.StopPolicy(max_resid=args.max_resid)
-    tiling = dict(chunk=16, rows=4, prefetch=1, group=0)
+    tiling = dict(zip(("chunk", "rows", "prefetch", "group", "streams"), (int(v) for v in args.shape.split(","))))
     metrics = {"policy": policy.__dict__, "arch": ES.ARCH}
     t0 = time.perf_counter()
     test_seeds = range(10000, 10000 + args.test)
@@ -231,7 +241,8 @@ def main():
     log(f"trained: {metrics['training']}")
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
-    metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling)
+    metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling,
+                                     traces_out=os.path.join(args.out, "es_test_traces.npz"))
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
     print(json.dumps(metrics["evaluation"]), flush=True)

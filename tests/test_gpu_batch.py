@@ -55,16 +55,19 @@ def solo(request):
     return request.param, states
 
 
-@pytest.mark.parametrize("chunk,rows,pf,group", [(8, 4, 1, 0), (3, 2, 2, 0), (1, 8, 1, 1), (5, 4, 1, 7),
-                                                 (16, 2, 2, 3), (8, 4, 3, 0), (4, 8, 4, 2)])
-def test_batch_matches_solo_runs(solo, chunk, rows, pf, group):
+@pytest.mark.parametrize("chunk,rows,pf,group,streams",
+                         [(8, 4, 1, 0, 0), (3, 2, 2, 0, 0), (1, 8, 1, 1, 0), (5, 4, 1, 7, 0), (16, 2, 2, 3, 0),
+                          (8, 4, 3, 0, 0), (4, 8, 4, 2, 0),
+                          # member-kernel mode: 1 stream, fewer streams than members, more streams than members
+                          (8, 4, 1, 0, 1), (3, 2, 2, 0, 3), (16, 4, 1, 0, 6), (8, 4, 3, 0, 2)])
+def test_batch_matches_solo_runs(solo, chunk, rows, pf, group, streams):
     precision, states = solo
     if pf > 2 and precision != "f32-table":
         pytest.skip("shared-memory stages are a material-table form")
     engs = [Engine(p, precision) for p in _members()]
     try:
-        with Batch(engs, chunk, rows, pf, group) as b:
-            assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group}
+        with Batch(engs, chunk, rows, pf, group, streams) as b:
+            assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams}
             b.run(STEPS)
             assert b.step == STEPS
         for q, e in enumerate(engs):
@@ -183,6 +186,57 @@ def test_batch_with_time_blocked_dft_matches_solo_runs():
             b.run(20)
         for q, e in enumerate(engs):
             _assert_same(solo[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_batch_modes_alternate_within_one_run_sequence():
+    """Tile-list and member-kernel runs of the same batch continue each other
+    (the step counters and blocked-DFT state carry over between the modes)."""
+    probs = [build_problem_from_scenario(s, 200, per_cell=False)
+             for s in (small_scenario(1, "xp"), small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3)),
+                       small_scenario(3, "zp", ncpml=(5, 4, 3, 3, 4, 5)))]
+    solo = []
+    for p in probs:
+        with Engine(p, "f32-table", dft_block=16) as e:
+            e.run(200)
+            solo.append(_state(e))
+    engs = [Engine(p, "f32-table", dft_block=16) for p in probs]
+    try:
+        with Batch(engs) as b:
+            b.run(30)                     # tile-list, no graph
+            b.set_tiling(8, 4, 1, 0, 2)
+            b.run(70)                     # member kernels: one graph replay + 6 steps
+            b.set_tiling(16, 2, 1, 0, 0)
+            b.run(64)                     # tile-list graph
+            b.set_tiling(32, 4, 1, 0, 3)
+            b.run(36)
+            assert b.step == 200
+        for q, e in enumerate(engs):
+            assert e.step == 200
+            _assert_same(solo[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_member_mode_watchdog_and_profile():
+    probs = _members(140)[:3]
+    probs[2].voltage_sources[0].voltage_per_e_field[100] = np.nan
+    engs = [Engine(p, "f32-table") for p in probs]
+    try:
+        with Batch(engs, 8, 4, 1, 0, 2) as b:
+            prof = b.profile_kernels(4)
+            assert all(v > 0 for v in prof.values())
+            with pytest.raises(N.FdtdError) as ei:
+                b.run(128)
+            assert ei.value.code == N.FDTD_ERR_NONFINITE
+            assert "member 2" in str(ei.value)
+            with pytest.raises(N.FdtdError):
+                b.set_tiling(8, 4, 1, 0, 33)
+        assert engs[2].status() == (N.FDTD_ERR_NONFINITE, 100)
+        assert engs[0].status() == (0, -1)
     finally:
         for e in engs:
             e.close()
