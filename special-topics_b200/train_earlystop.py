@@ -101,8 +101,8 @@ def plain_reference(ES, pool, seeds, policy, tiling, group=64):
         try:
             t0 = time.perf_counter()
             with Batch(engs) as b:
-                if tiling:
-                    b.set_shape(tiling)
+                if tiling:   # shared-memory stages (prefetch 3, 4) are a material-table form
+                    b.set_shape(dict(tiling, prefetch=min(tiling.get("prefetch", 1), 2)))
                 b.run(policy.n_total)
             for e in engs:
                 ref.append(ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs))
