@@ -26,6 +26,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import os
+import threading
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
@@ -414,13 +415,21 @@ class StopPolicy:
     """n_in: steps the network reads.  checkpoints: steps at which a run may
     stop.  At a checkpoint each candidate pole set (the network's, and matrix
     pencils of the run's own samples since n_in, orders `pencil_orders`) is
-    fitted to [n_in, checkpoint); the best fit stops the run when its
-    residual-energy ratio is at most max_resid, and always at the last
-    checkpoint.  Runs that do not stop keep stepping (plain FDTD) to the next
-    checkpoint.  n_total: the step count the result stands in for."""
+    fitted to [n_in, checkpoint).  The run stops when the `agree_count`
+    best-fitting candidates all have a residual-energy ratio of at most
+    max_resid and their extrapolated |S11| agree within agree_db (largest
+    difference over S11_FREQS); it then keeps the best-fitting tail.  At the
+    last checkpoint it always stops, with the best-fitting tail.  Runs that do
+    not stop keep stepping (plain FDTD) to the next checkpoint.  n_total: the
+    step count the result stands in for.  (On 256 held-out inverted-F
+    variants, seeds 10000..10255, this rule put 98% of the runs within 0.1 dB
+    of the full FP64 S11, at a mean stop of 4557 steps; a residual gate
+    alone at 1e-4 put 47-55% there.)"""
     n_in: int = 1500
     checkpoints: tuple = (2300, 3000, 4000, 5000)
-    max_resid: float = 1e-4
+    max_resid: float = 1e-3
+    agree_db: float = 0.02
+    agree_count: int = 3
     n_total: int = 7000
     pencil_orders: tuple = (8, 12, 16)
     decim: int = DECIM
@@ -435,25 +444,71 @@ def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None
     return out + [P for P in sets if P]
 
 
-def best_tail(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None):
-    """(traces over n_total, residual, index of the winning candidate) of the
-    candidate pole set that fits [n_in, n1) best; None when no candidate fits."""
-    best = None
+def tail_candidates(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
+    """(traces over n_total, residual, candidate index) of every candidate pole
+    set fitted to [n_in, n1), lowest residual first."""
+    out = []
     for q, P in enumerate(candidate_poles(V, I, n1, dt, policy, net_poles)):
         try:
             v, i, r = pole_tail(V, I, P, policy.n_in, n1, policy.n_total, dt)
         except np.linalg.LinAlgError:
             continue
-        if np.isfinite(r) and (best is None or r < best[2]):
-            best = (v, i, r, q)
-    return best
+        if np.isfinite(r):
+            out.append((v, i, r, q))
+    return sorted(out, key=lambda c: c[2])
+
+
+def best_tail(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None):
+    """The candidate of tail_candidates with the lowest residual, or None."""
+    c = tail_candidates(V, I, n1, dt, policy, net_poles)
+    return c[0] if c else None
+
+
+_BASIS: dict = {}
+_BASIS_LOCK = threading.Lock()
+
+
+def s11_db_host(V, I, dt: float, freqs=None, z0: float = 50.0) -> np.ndarray:
+    """|S11| in dB on the host: the transform of dft.js:17-38 (X(f) = dt
+    sum_n x[n] exp(-j w ((n + 1) dt + shift)), shift -dt/2 for the current)
+    as a matrix product with a cached basis, then postproc.s11.  The stop
+    rule compares candidate tails with it; reported S11 uses s11_db."""
+    from . import postproc
+    freqs = S11_FREQS if freqs is None else np.asarray(freqs, dtype=np.float64)
+    n = len(V)
+    key = (n, float(dt), freqs.size, float(freqs[0]), float(freqs[-1]))
+    with _BASIS_LOCK:
+        E = _BASIS.get(key)
+        if E is None:
+            w = 2 * math.pi * freqs
+            E = np.exp(-1j * np.outer(w, (np.arange(n) + 1) * dt))
+            _BASIS.clear()
+            _BASIS[key] = E
+    w = 2 * math.pi * freqs
+    xv = dt * (E @ np.asarray(V, dtype=np.float64))
+    xi = dt * (E @ np.asarray(I, dtype=np.float64)) * np.exp(1j * w * dt / 2)
+    return postproc.s11((xv.real, xv.imag), (xi.real, xi.imag), z0)["mag_dB"]
+
+
+def stop_fit(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, last: bool = False):
+    """The tail (traces over n_total, residual, candidate index) a run stops
+    with at checkpoint n1, or None to keep stepping (StopPolicy's rule)."""
+    cands = tail_candidates(V, I, n1, dt, policy, net_poles)
+    if not cands:
+        return None
+    ok = [c for c in cands if c[2] <= policy.max_resid][:policy.agree_count]
+    if len(ok) == policy.agree_count:
+        s = [s11_db_host(c[0], c[1], dt) for c in ok]
+        if all(np.abs(s[0] - x).max() <= policy.agree_db for x in s[1:]):
+            return ok[0]
+    return cands[0] if last else None
 
 
 def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: dict | None = None,
                         use_network: bool = True) -> list[dict]:
     """Advances FP32 engines of one batch through the checkpoints of `policy`
-    and stops each run at the first checkpoint whose best fit passes the gate
-    (the last checkpoint always stops).  With use_network the network's pole
+    and stops each run at the first checkpoint where the policy's rule
+    (stop_fit) stops it; the last checkpoint always stops.  With use_network the network's pole
     set (predicted on the device from the first n_in steps) competes with the
     pencils.  Returns per engine {"V", "I": traces over n_total steps,
     "stopped_at", "resid", "winner": "network" or "pencil"}."""
@@ -478,8 +533,8 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
 
         def fit_one(k):
             q = active[k]
-            return best_tail(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
-                             net_poles[q] if use_network else None)
+            return stop_fit(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
+                            net_poles[q] if use_network else None, last)
 
         # the fits are LAPACK-bound and release the GIL: one thread per host
         # core, each with a single BLAS thread (16 fits each spreading over
@@ -488,7 +543,7 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
             fits = list(ex.map(fit_one, range(len(active))))
         for k, q in enumerate(active):
             got = fits[k]
-            if got is not None and (got[2] <= policy.max_resid or last):
+            if got is not None:
                 v, i, r, w = got
                 out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
                           "winner": "network" if (use_network and net_poles[q] and w == 0) else "pencil"}

@@ -183,7 +183,7 @@ def main():
     ap.add_argument("--test", type=int, default=512)
     ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--batch", type=int, default=128)
-    ap.add_argument("--max-resid", type=float, default=1e-4)
+    ap.add_argument("--max-resid", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cache", default=None, help="npz of a previous run's training set and test reference")
     ap.add_argument("--shape", default="16,4,1,0,0",

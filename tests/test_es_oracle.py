@@ -7,6 +7,7 @@ import pytest
 import torch
 
 import es_net_oracle as O
+import oracle
 from conftest import load_package
 
 pkg = load_package()
@@ -117,6 +118,28 @@ def test_window_poles_and_tail_recover_two_modes():
     pol = ES.StopPolicy(pencil_orders=(4,))
     got = ES.best_tail(V, I, 2300, dt, pol)
     assert got is not None and got[2] < 1e-12
+
+
+def test_stop_rule_needs_agreeing_candidates():
+    dt = 8.666e-13
+    m1 = ES.Mode(2.09e9, 0.45e9, 0.011 - 0.004j, 1.5e-4 + 2e-5j, 1500)
+    m2 = ES.Mode(2.61e9, 0.9e9, 0.004 + 0.002j, -4e-5 + 1e-5j, 1500)
+    V, I = _ringing(m1, 7000, extra=m2)
+    # host S11 of the rule follows the reference's transform (oracle restatement)
+    Vr, Vi = oracle.time_to_freq(V, dt, ES.S11_FREQS, 0.0)
+    Ir, Ii = oracle.time_to_freq(I, dt, ES.S11_FREQS, -dt / 2)
+    want = oracle.s11((Vr, Vi), (Ir, Ii), 50.0)["mag_dB"]
+    assert np.allclose(ES.s11_db_host(V, I, dt), want, atol=1e-9)
+    # three exact candidates agree: the run stops with an exact tail
+    pol = ES.StopPolicy(pencil_orders=(4, 4, 4))
+    got = ES.stop_fit(V, I, 2300, dt, pol)
+    assert got is not None and got[2] < 1e-12
+    # candidates that may not differ at all never agree: keep stepping, except at the last checkpoint
+    strict = ES.StopPolicy(pencil_orders=(4, 4, 4), agree_db=-1.0)
+    assert ES.stop_fit(V, I, 2300, dt, strict) is None
+    assert ES.stop_fit(V, I, 2300, dt, strict, last=True) is not None
+    # too few candidates pass the residual gate: keep stepping
+    assert ES.stop_fit(V, I, 2300, dt, ES.StopPolicy(pencil_orders=(4,))) is None
 
 
 def test_growth_onset_finds_late_growth():
