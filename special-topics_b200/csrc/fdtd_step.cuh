@@ -718,6 +718,20 @@ __device__ __forceinline__ void h_lean_range(const StepParams<T, C>& p, const HC
                                              T& ey_c) {
   if constexpr (PF >= 3 && C::kTable) {
     h_staged_range<PF>(p, c, xa, xb, ez_c, ey_c);
+  } else if (PF == 1 && xa < xb) {
+    // software pipeline, depth 1, as two alternating register sets: the next
+    // plane's loads are in flight while plane i is computed and stored, and
+    // no set is copied into the other
+    HIn<T, C> a, b;
+    h_load(p, c, xa, a);
+    int i = xa;
+    for (; i + 1 < xb; i += 2) {
+      h_load(p, c, i + 1, b);
+      h_store<T, C, EXACT>(p, c, i, a, ez_c, ey_c);
+      if (i + 2 < xb) h_load(p, c, i + 2, a);
+      h_store<T, C, EXACT>(p, c, i + 1, b, ez_c, ey_c);
+    }
+    if (i < xb) h_store<T, C, EXACT>(p, c, i, a, ez_c, ey_c);
   } else if (xa < xb) {
     // software pipeline: the loads of the next PF planes are in flight while
     // plane i is computed and stored
@@ -1268,6 +1282,18 @@ __device__ __forceinline__ void e_lean_range(const StepParams<T, C>& p, const EC
                                              T& hy_p) {
   if constexpr (PF >= 3 && C::kTable) {
     e_staged_range<PF>(p, c, xa, xb, hz_p, hy_p);
+  } else if (PF == 1 && xa < xb) {
+    // depth 1 as two alternating register sets (see h_lean_range)
+    EIn<T, C> a, b;
+    e_load(p, c, xa, a);
+    int i = xa;
+    for (; i + 1 < xb; i += 2) {
+      e_load(p, c, i + 1, b);
+      e_store<T, C, EXACT>(p, c, i, a, hz_p, hy_p);
+      if (i + 2 < xb) e_load(p, c, i + 2, a);
+      e_store<T, C, EXACT>(p, c, i + 1, b, hz_p, hy_p);
+    }
+    if (i < xb) e_store<T, C, EXACT>(p, c, i, a, hz_p, hy_p);
   } else if (xa < xb) {
     EIn<T, C> cur, nxt, nx2;
     e_load(p, c, xa, cur);

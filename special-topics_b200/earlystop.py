@@ -516,44 +516,73 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
     out = [None] * len(engines)
     net_poles = [None] * len(engines)
     active = list(range(len(engines)))
-    for cp in policy.checkpoints:
-        with Batch([engines[q] for q in active]) as b:
-            if tiling:
-                b.set_shape(tiling)
-            b.run(cp - b.step)
-        if use_network and net is not None and net_poles[active[0]] is None:
-            sub = [engines[q] for q in active]
-            for g0 in range(0, len(sub), net.max_batch):
-                y, _ = net.predict_members(sub[g0:g0 + net.max_batch], policy.decim)
-                for k, q in enumerate(active[g0:g0 + net.max_batch]):
-                    net_poles[q] = target_to_poles(y[k])
-        rest = []
-        last = cp == policy.checkpoints[-1]
-        traces = [(engines[q].voltages(cp)[0], engines[q].currents(cp)[0]) for q in active]
+    cps = list(policy.checkpoints)
 
-        def fit_one(k):
-            q = active[k]
-            return stop_fit(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
-                            net_poles[q] if use_network else None, last)
+    def batch_of(qs):
+        bt = Batch([engines[q] for q in qs])
+        if tiling:
+            bt.set_shape(tiling)
+        return bt
 
-        # the fits are LAPACK-bound and release the GIL: one thread per host
-        # core, each with a single BLAS thread (16 fits each spreading over
-        # every core oversubscribe the host many times over)
-        with threadpool_limits(limits=1), ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
-            fits = list(ex.map(fit_one, range(len(active))))
-        for k, q in enumerate(active):
-            got = fits[k]
-            if got is not None:
-                v, i, r, w = got
-                out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
-                          "winner": "network" if (use_network and net_poles[q] and w == 0) else "pencil"}
-            else:                          # keeps stepping (at the last checkpoint: to n_total)
-                rest.append(q)
-        if cp == policy.checkpoints[-1]:
-            break
-        active = rest
-        if not active:
-            break
+    b = batch_of(active)
+    try:
+        b.run(cps[0] - b.step)
+        for n, cp in enumerate(cps):
+            last = n == len(cps) - 1
+            if use_network and net is not None and n == 0:
+                sub = [engines[q] for q in active]
+                for g0 in range(0, len(sub), net.max_batch):
+                    y, _ = net.predict_members(sub[g0:g0 + net.max_batch], policy.decim)
+                    for k, q in enumerate(active[g0:g0 + net.max_batch]):
+                        net_poles[q] = target_to_poles(y[k])
+            traces = [(engines[q].voltages(cp)[0], engines[q].currents(cp)[0]) for q in active]
+            # While the host fits this checkpoint, the GPU steps every active
+            # run on to the next one (the library call releases the GIL).  The
+            # runs that stop here are stepped for nothing, which costs less
+            # than leaving the GPU idle during the fits.
+            ahead, err = None, []
+            if not last:
+                def step_ahead(bt=b, count=cps[n + 1] - cp):
+                    try:
+                        bt.run(count)
+                    except Exception as e:  # re-raised on this thread after the fits
+                        err.append(e)
+                ahead = threading.Thread(target=step_ahead)
+                ahead.start()
+
+            def fit_one(k):
+                q = active[k]
+                return stop_fit(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
+                                net_poles[q] if use_network else None, last)
+
+            # the fits are LAPACK-bound and release the GIL: one thread per host
+            # core, each with a single BLAS thread (16 fits each spreading over
+            # every core oversubscribe the host many times over)
+            try:
+                with threadpool_limits(limits=1), ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+                    fits = list(ex.map(fit_one, range(len(active))))
+            finally:
+                if ahead is not None:
+                    ahead.join()
+            if err:
+                raise err[0]
+            rest = []
+            for k, q in enumerate(active):
+                got = fits[k]
+                if got is not None:
+                    v, i, r, w = got
+                    out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
+                              "winner": "network" if (use_network and net_poles[q] and w == 0) else "pencil"}
+                else:                      # keeps stepping (at the last checkpoint: to n_total)
+                    rest.append(q)
+            if last or not rest:
+                break
+            if len(rest) != len(active):   # the rest are at the next checkpoint already
+                b.close()
+                b = batch_of(rest)
+            active = rest
+    finally:
+        b.close()
     leftover = [q for q in range(len(engines)) if out[q] is None]
     if leftover:
         with Batch([engines[q] for q in leftover]) as b:

@@ -240,3 +240,34 @@ def test_member_mode_watchdog_and_profile():
     finally:
         for e in engs:
             e.close()
+
+
+def test_early_stop_driver_keeps_each_runs_own_traces():
+    """The checkpoint driver steps the batch to the next checkpoint while it
+    fits the current one, and rebuilds the batch when runs stop: every run's
+    traces up to its stop step are still those of the same run stepped alone."""
+    from special_topics_b200 import earlystop as ES
+    steps = 160
+    probs = _members(steps)[:3]
+    solo = []
+    for p in probs:
+        with Engine(p, "f32-table") as e:
+            e.run(steps)
+            solo.append((e.voltages()[0], e.currents()[0]))
+    for policy in (ES.StopPolicy(n_in=40, checkpoints=(70, 100, 130), n_total=steps, pencil_orders=(4, 6, 8),
+                                 decim=1, max_resid=1.0, agree_db=1e9),      # stops at the first fit
+                   ES.StopPolicy(n_in=40, checkpoints=(70, 100, 130), n_total=steps, pencil_orders=(4, 6, 8),
+                                 decim=1, agree_db=-1.0)):                    # stops at the last checkpoint
+        engs = [Engine(p, "f32-table") for p in probs]
+        try:
+            res = ES.run_with_early_stop(engs, None, policy, {"chunk": 8, "rows": 4}, use_network=False)
+        finally:
+            for e in engs:
+                e.close()
+        for q, r in enumerate(res):
+            # the strict rule never sees agreement: nothing stops before the last checkpoint
+            assert r["stopped_at"] in ((70, 100, 130, steps) if policy.agree_db > 0 else (130, steps))
+            assert r["V"].shape == (steps,) and r["I"].shape == (steps,)
+            n = r["stopped_at"]
+            assert np.array_equal(r["V"][:n], solo[q][0][:n])
+            assert np.array_equal(r["I"][:n], solo[q][1][:n])
