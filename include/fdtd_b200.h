@@ -116,7 +116,12 @@ int fdtd_ctx_upload_coeff(fdtd_ctx* ctx, int which, const double* host, long n);
  * CPsi slot arrays in the reference's Psi layouts, and the first H / E index of
  * the face along its axis.  kappa_e / kappa_m (length nc, may be NULL for the
  * per-cell problems) are needed by FDTD_PREC_F32_TABLE problems, whose
- * coefficient tables carry no kappa division. */
+ * coefficient tables carry no kappa division.  An FP64 problem whose
+ * coefficients came from fdtd_ctx_build_material passes no CPsi (all four
+ * pointers NULL, counts 0) and the kappa profiles instead: the device then
+ * takes CPsi from the coefficients and divides the face's band of them by
+ * kappa, as cpml.js:212-243 does, once per face, in the order the faces are
+ * uploaded. */
 int fdtd_ctx_upload_cpml(fdtd_ctx* ctx, int faceId, int nc, const double* b_e, const double* a_e,
                          const double* b_m, const double* a_m, const double* kappa_e, const double* kappa_m,
                          const double* CPsi0, long n0, const double* CPsi1, long n1, const double* CPsi2,
@@ -151,7 +156,10 @@ int fdtd_ctx_setup_farfield(fdtd_ctx* ctx, int nFreq, const double* freqs, int l
 int fdtd_ctx_upload_material(fdtd_ctx* ctx, int comp, const unsigned char* ids, long n, const double* table,
                              int rows);
 
-/* Material-table problem built on the device from the material grid
+/* Coefficients built on the device from the material grid, for
+ * FDTD_PREC_F32_TABLE problems (ids and tables) and FDTD_PREC_F64 problems (the
+ * 18 per-cell arrays, bit-identical to the reference's arithmetic, before the
+ * CPML kappa division, which fdtd_ctx_upload_cpml then applies)
  * (materials.js:21-332 + coefficients.js:22-116): `mat` holds one type id per
  * cell (nx*ny*nz, k fastest; 1-based ids as materials.js stores them), `props`
  * has 4 values per type id 0..ntypes-1 (eps_r, mu_r, sigma_e, sigma_m, with
@@ -164,7 +172,8 @@ int fdtd_ctx_build_material(fdtd_ctx* ctx, const unsigned char* mat, long ncells
 
 /* Gives `count` cells of component comp (API order Ex Ey Ez Hx Hy Hz) their own
  * coefficient triples (self, curl1, curl2), e.g. the lumped-source cells of
- * coefficients.js:158-207. */
+ * coefficients.js:158-207: new table rows for FDTD_PREC_F32_TABLE problems,
+ * the three per-cell arrays of comp for FDTD_PREC_F64 problems. */
 int fdtd_ctx_override_material(fdtd_ctx* ctx, int comp, const int* idx, const double* triples, int count);
 
 /* Reads back a component's ids and its coefficient table (FP64, rows x 3). */

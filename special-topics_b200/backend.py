@@ -68,7 +68,8 @@ class Engine:
             for comp_id, (ids, tab) in enumerate(build_tables(p)[c] for c in COMPONENTS):
                 N.check(L.fdtd_ctx_upload_material(h, comp_id, ids.ctypes.data_as(C.POINTER(C.c_ubyte)),
                                                    ids.size, N.dptr(tab.ravel()), tab.shape[0]))
-        elif table:
+        elif table or (self.precision == "f64" and not p.coeffs):
+            # FP64 problems built without per-cell arrays get them on the device
             self._build_tables_on_device()
         else:
             for w, name in enumerate(COEFF_ORDER):
@@ -80,7 +81,7 @@ class Engine:
             prof = [np.ascontiguousarray(x, dtype=np.float64)
                     for x in (f.b_e, f.a_e, f.b_m, f.a_m, f.kappa_e, f.kappa_m)]
             args = []
-            for cp in (f.cpsi if not table else [None] * 4):
+            for cp in (f.cpsi if (not table and f.cpsi is not None) else [None] * 4):
                 if cp is None:
                     args += [None, 0]
                 else:
@@ -106,6 +107,10 @@ class Engine:
             N.check(L.fdtd_ctx_setup_farfield(h, fr.size, N.dptr(fr), ff.li, ff.lj, ff.lk, ff.ui, ff.uj, ff.uk))
 
     def _build_tables_on_device(self) -> None:
+        """Material tables (FP32-table), or the 18 per-cell FP64 coefficient
+        arrays, from the problem's material grid on the device, then the
+        lumped-source cells' own triples.  (For FP64 the CPML kappa division
+        follows when the faces are uploaded without CPsi.)"""
         L, p, h = N.lib(), self.problem, self._h
         mat = np.ascontiguousarray(p.meta["material_grid"], dtype=np.uint8).ravel()
         props = np.ascontiguousarray(p.meta["material_props"], dtype=np.float64)

@@ -90,6 +90,8 @@ struct fdtd_ctx {
   void* fields = nullptr;   // contiguous Hx..Ez (+ slack)
   void* coef[18] = {};
   bool coef_set[18] = {};
+  bool coef_device = false;     // FP64 coefficients built by fdtd_ctx_build_material
+  bool kappa_done[6] = {};      // face whose CPML band of them was divided by kappa on the device
   // material-table problem
   unsigned char* ids[6] = {};
   bool ids_set[6] = {};
@@ -724,6 +726,43 @@ int fdtd_ctx_upload_coeff(fdtd_ctx* c, int which, const double* host, long n) {
   CK(cudaSetDevice(c->device));
   int rc = upload_real(c, c->coef[which], host, n);
   if (!rc) c->coef_set[which] = true;
+  c->coef_device = false;  // host arrays carry their own kappa division and come with CPsi
+  return rc;
+}
+
+// The CPML bands of face f on the four per-cell FP64 coefficient arrays its
+// Psi slots correct (cpml.js:212-243): per slot, CPsi = coefficient x cell size
+// over the band (into the face's CPsi array), then the coefficient is divided
+// by kappa of its band cell.  Slots: x face Chyez Chzey Ceyhz Cezhy, y face
+// Chxez Chzex Cezhx Cexhz, z face Chxey Chyex Cexhy Ceyhx (ids as in
+// fdtd_ctx_upload_coeff); the H slots use the H band and kappa_m, the E slots
+// the E band and kappa_e.
+static int cpml_band_on_device(fdtd_ctx* c, int f, const double* kappa_e, const double* kappa_m) {
+  static const int coef_id[3][4] = {{13, 17, 5, 7}, {11, 16, 8, 1}, {10, 14, 2, 4}};
+  const int axis = f / 2;
+  HostFace& h = c->face[f];
+  const double cell = axis == 0 ? c->dx : (axis == 1 ? c->dy : c->dz);
+  double* d_kap = nullptr;
+  if (cudaMalloc((void**)&d_kap, 2 * h.nc * sizeof(double)) != cudaSuccess) return fail(FDTD_ERR_OOM, "kappa profiles");
+  int rc = FDTD_OK;
+  if (xfer(c, d_kap, kappa_e, h.nc * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      xfer(c, d_kap + h.nc, kappa_m, h.nc * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(FDTD_ERR_CUDA, "kappa upload");
+  for (int s = 0; s < 4 && !rc; s++) {
+    const int id = coef_id[axis][s], comp = id / 3;   // API order Ex Ey Ez Hx Hy Hz
+    const int ni = (comp == 0 || comp == 4 || comp == 5) ? c->nx : c->nx + 1;
+    const int nj = (comp == 1 || comp == 3 || comp == 5) ? c->ny : c->ny + 1;
+    const int nk = (comp == 2 || comp == 3 || comp == 4) ? c->nz : c->nz + 1;
+    const int st = s < 2 ? h.m_start : h.e_start;
+    const long long n = (long long)(axis == 0 ? h.nc : ni) * (axis == 1 ? h.nc : nj) * (axis == 2 ? h.nc : nk);
+    if (n != h.n[s]) { rc = fail(FDTD_ERR_STATE, "face %d slot %d: band of %lld cells, Psi of %lld", f, s, n, h.n[s]); break; }
+    k_cpml_band<<<148 * 8, 256, 0, c->stream>>>((double*)c->coef[id], ni, nj, nk, axis, st, h.nc, cell,
+                                                s < 2 ? d_kap + h.nc : d_kap, (double*)h.cpsi[s]);
+  }
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess)
+    rc = fail(FDTD_ERR_CUDA, "CPML band: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFree(d_kap);
+  if (!rc) c->kappa_done[f] = true;
   return rc;
 }
 
@@ -745,8 +784,17 @@ int fdtd_ctx_upload_cpml(fdtd_ctx* c, int f, int nc, const double* b_e, const do
   psi_sizes(c, f, nc, want);
   const double* cp[4] = {CPsi0, CPsi1, CPsi2, CPsi3};
   const long got[4] = {n0, n1, n2, n3};
+  // FP64 coefficients built on the device and no CPsi given: CPsi and the
+  // kappa division of the band are done here, on the device
+  const bool dev = !table && c->coef_device && !CPsi0 && !CPsi1 && !CPsi2 && !CPsi3 && !n0 && !n1 && !n2 && !n3;
+  if (dev && nc > 0) {
+    if (!kappa_e || !kappa_m) return fail(FDTD_ERR_BADARG, "face %d: device-built coefficients need kappa profiles", f);
+    if (c->kappa_done[f]) return fail(FDTD_ERR_STATE, "face %d: its band was already divided by kappa; rebuild the coefficients first", f);
+    for (int q = 0; q < nc; q++)
+      if (!(kappa_e[q] > 0) || !(kappa_m[q] > 0)) return fail(FDTD_ERR_BADARG, "face %d: kappa must be positive", f);
+  }
   for (int s = 0; s < 4; s++) {
-    if (table) continue;  // CPsi comes from the coefficient tables
+    if (table || dev) continue;  // CPsi comes from the coefficient tables, or is made on the device
     if (got[s] != want[s] || (want[s] > 0 && !cp[s]))
       return fail(FDTD_ERR_BADARG, "face %d slot %d: got %ld CPsi values, expected %lld", f, s, got[s], want[s]);
   }
@@ -770,9 +818,10 @@ int fdtd_ctx_upload_cpml(fdtd_ctx* c, int f, int nc, const double* b_e, const do
     rc = dalloc(c, &h.psi[s], want[s] * c->esz);
     if (!rc && !table) {
       rc = dalloc(c, &h.cpsi[s], want[s] * c->esz);
-      if (!rc) rc = upload_real(c, h.cpsi[s], cp[s], want[s]);
+      if (!rc && !dev) rc = upload_real(c, h.cpsi[s], cp[s], want[s]);
     }
   }
+  if (!rc && dev) rc = cpml_band_on_device(c, f, kappa_e, kappa_m);
   if (!rc && table) {
     std::vector<float> ik(nc);
     const double* kp[2] = {kappa_e, kappa_m};
@@ -966,7 +1015,9 @@ static int set_rows(fdtd_ctx* c, int comp, const std::vector<double>& rows) {
 int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, int ntypes, const double* props,
                             int nplates, const int* plates, const double* plate_sigma) {
   if (!c || !mat || !props || (nplates > 0 && (!plates || !plate_sigma))) return fail(FDTD_ERR_BADARG, "NULL argument");
-  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table problem");
+  if (c->prec == FDTD_PREC_F32)
+    return fail(FDTD_ERR_STATE, "per-cell FP32 problems take fdtd_ctx_upload_coeff (FP64 and material-table problems build here)");
+  const bool f64 = c->prec == FDTD_PREC_F64;
   if (ncells != (long)c->nx * c->ny * c->nz) return fail(FDTD_ERR_BADARG, "material grid of %ld cells, need %lld", ncells, (long long)c->nx * c->ny * c->nz);
   if (ntypes < 1 || ntypes > 48) return fail(FDTD_ERR_BADARG, "%d material slots (1..48 supported)", ntypes);
   if (nplates < 0 || nplates > kMaxPlates) return fail(FDTD_ERR_BADARG, "%d plates (at most %d)", nplates, kMaxPlates);
@@ -992,12 +1043,15 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
   CK(cudaSetDevice(c->device));
   unsigned char* d_mat = nullptr;
   uint8_t *d_present = nullptr, *d_map = nullptr;
+  int* d_map64 = nullptr;     // FP64: code -> row
+  double* d_rows = nullptr;   // FP64: row triples
   const long long M = ntypes;
   const long long ncode_e = (M * M * M * M + 1) * (long long)(psig.size() + 1);
   const long long ncode_h = M * M + 1;
   int rc = FDTD_OK;
   if (cudaMalloc(&d_mat, ncells) != cudaSuccess || cudaMalloc(&d_present, std::max(ncode_e, ncode_h)) != cudaSuccess ||
-      cudaMalloc(&d_map, std::max(ncode_e, ncode_h)) != cudaSuccess) {
+      cudaMalloc(&d_map, std::max(ncode_e, ncode_h)) != cudaSuccess ||
+      (f64 && cudaMalloc((void**)&d_map64, std::max(ncode_e, ncode_h) * sizeof(int)) != cudaSuccess)) {
     rc = fail(FDTD_ERR_OOM, "material build buffers");
   }
   if (!rc && xfer(c, d_mat, mat, ncells, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "material grid upload");
@@ -1016,6 +1070,7 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
     }
     std::map<std::pair<double, double>, int> rowof;
     std::vector<double> rows;
+    std::vector<int> row_of_code(f64 ? ncode : 0, 0);
     map.assign(ncode, 0);
     const long long fill = comp < 3 ? M * M * M * M : M * M;
     for (long long code = 0; code < ncode; code++) {
@@ -1053,6 +1108,27 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
         r = it->second;
       }
       map[code] = (uint8_t)std::min(r, 255);
+      if (f64) row_of_code[code] = r;
+    }
+    if (f64) {
+      // every cell takes its row's FP64 triple: coefficient arrays 3 comp .. 3 comp + 2
+      const std::vector<int>& map64 = row_of_code;
+      cudaFree(d_rows);
+      d_rows = nullptr;
+      if (cudaMalloc((void**)&d_rows, std::max<size_t>(rows.size(), 1) * sizeof(double)) != cudaSuccess) {
+        rc = fail(FDTD_ERR_OOM, "coefficient rows");
+        break;
+      }
+      if (xfer(c, d_rows, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+          xfer(c, d_map64, map64.data(), ncode * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = fail(FDTD_ERR_CUDA, "coefficient row upload");
+        break;
+      }
+      k_material_coef<<<148 * 8, 256, 0, c->stream>>>(b, comp, d_map64, d_rows, (double*)c->coef[3 * comp],
+                                                      (double*)c->coef[3 * comp + 1], (double*)c->coef[3 * comp + 2]);
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = fail(FDTD_ERR_CUDA, "coefficients: %s", cudaGetErrorString(cudaGetLastError())); break; }
+      for (int w = 0; w < 3; w++) c->coef_set[3 * comp + w] = true;
+      continue;
     }
     rc = set_rows(c, comp, rows);
     if (rc) break;
@@ -1064,13 +1140,54 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
   cudaFree(d_mat);
   cudaFree(d_present);
   cudaFree(d_map);
+  cudaFree(d_map64);
+  cudaFree(d_rows);
+  if (f64) {
+    c->coef_device = rc == FDTD_OK;
+    for (int f = 0; f < 6; f++) c->kappa_done[f] = false;
+  }
+  invalidate(c);
+  return rc;
+}
+
+// FP64 problems: the triples overwrite coefficient arrays 3 comp .. 3 comp + 2 at the cells.
+static int override_coef64(fdtd_ctx* c, int comp, const int* idx, const double* triples, int count) {
+  if (comp < 0 || comp > 5) return fail(FDTD_ERR_BADARG, "component %d not in 0..5", comp);
+  for (int w = 0; w < 3; w++)
+    if (!c->coef_set[3 * comp + w]) return fail(FDTD_ERR_STATE, "component %d has no coefficients yet", comp);
+  if (count <= 0) return FDTD_OK;
+  const long long n = coef_count(c, 3 * comp);
+  for (int q = 0; q < count; q++) {
+    if (idx[q] < 0 || idx[q] >= n) return fail(FDTD_ERR_BADARG, "cell index %d out of range", idx[q]);
+    for (int w = 0; w < 3; w++)
+      if (!std::isfinite(triples[3 * q + w])) return fail(FDTD_ERR_BADARG, "non-finite coefficient");
+  }
+  CK(cudaSetDevice(c->device));
+  int* d_idx = nullptr;
+  double* d_trip = nullptr;
+  int rc = FDTD_OK;
+  if (cudaMalloc((void**)&d_idx, count * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&d_trip, 3 * count * sizeof(double)) != cudaSuccess)
+    rc = fail(FDTD_ERR_OOM, "override buffers");
+  if (!rc && (xfer(c, d_idx, idx, count * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+              xfer(c, d_trip, triples, 3 * count * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess))
+    rc = fail(FDTD_ERR_CUDA, "override upload");
+  if (!rc) {
+    k_coef_override<<<1, 1, 0, c->stream>>>((double*)c->coef[3 * comp], (double*)c->coef[3 * comp + 1],
+                                            (double*)c->coef[3 * comp + 2], d_idx, d_trip, count);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+      rc = fail(FDTD_ERR_CUDA, "override: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  cudaFree(d_idx);
+  cudaFree(d_trip);
   invalidate(c);
   return rc;
 }
 
 int fdtd_ctx_override_material(fdtd_ctx* c, int comp, const int* idx, const double* triples, int count) {
   if (!c || !idx || !triples) return fail(FDTD_ERR_BADARG, "NULL argument");
-  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table problem");
+  if (c->prec == FDTD_PREC_F64) return override_coef64(c, comp, idx, triples, count);
+  if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table or FP64 problem");
   if (comp < 0 || comp > 5 || !c->ids_set[comp]) return fail(FDTD_ERR_STATE, "component %d has no material ids yet", comp);
   const long long n = c->ncomp[(comp + 3) % 6];
   std::vector<double> rows = c->rows64[comp];

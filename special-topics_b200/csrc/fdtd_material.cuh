@@ -90,4 +90,53 @@ __global__ void __launch_bounds__(256) k_material_ids(MatBuild b, int comp, cons
   }
 }
 
+// FP64 per-cell coefficients (the drop-in path built on the device): each
+// cell of component `comp` takes the FP64 triple of its code's row, computed
+// on the host with the reference's formulas (coefficients.js:22-116); out[w]
+// is coefficient array 3 * comp + w.
+__global__ void __launch_bounds__(256) k_material_coef(MatBuild b, int comp, const int* code_to_row,
+                                                       const double* rows, double* out0, double* out1, double* out2) {
+  int ni, nj, nk;
+  comp_extent(b, comp, ni, nj, nk);
+  const long long n = (long long)ni * nj * nk;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % nk), j = (int)((t / nk) % nj), i = (int)(t / ((long long)nj * nk));
+    const long long r = code_to_row[material_code(b, comp, i, j, k)];
+    out0[t] = rows[3 * r];
+    out1[t] = rows[3 * r + 1];
+    out2[t] = rows[3 * r + 2];
+  }
+}
+
+// The CPML band of one face on one per-cell FP64 coefficient array (an array
+// of extent ni x nj x nk; the band is [st, st + nc) along `axis`), as
+// cpml.js:212-243 does it: CPsi (the slot's array, C order over the band) is
+// the coefficient times the cell size, taken before the coefficient is divided
+// by kappa of its band cell.
+__global__ void __launch_bounds__(256) k_cpml_band(double* coef, int ni, int nj, int nk, int axis, int st, int nc,
+                                                   double cell, const double* kappa, double* cpsi) {
+  const int bi = axis == 0 ? nc : ni, bj = axis == 1 ? nc : nj, bk = axis == 2 ? nc : nk;
+  const long long n = (long long)bi * bj * bk;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % bk), b = (int)((t / bk) % bj), a = (int)(t / ((long long)bj * bk));
+    const int i = a + (axis == 0 ? st : 0), j = b + (axis == 1 ? st : 0), k = c + (axis == 2 ? st : 0);
+    const long long idx = ((long long)i * nj + j) * nk + k;
+    const double v = coef[idx];
+    cpsi[t] = __dmul_rn(v, cell);
+    coef[idx] = __ddiv_rn(v, kappa[axis == 0 ? a : (axis == 1 ? b : c)]);
+  }
+}
+
+// Source cells of an FP64 problem: their coefficient triples replace the
+// material ones (coefficients.js:158-207).  One thread, in list order, so a
+// repeated index keeps its last triple as the reference's assignment does.
+__global__ void k_coef_override(double* out0, double* out1, double* out2, const int* idx, const double* trip, int n) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int q = 0; q < n; q++) {
+    out0[idx[q]] = trip[3 * q];
+    out1[idx[q]] = trip[3 * q + 1];
+    out2[idx[q]] = trip[3 * q + 2];
+  }
+}
+
 }  // namespace fdtd

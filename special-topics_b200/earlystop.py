@@ -304,9 +304,10 @@ def _variant_problem(args):
 
 def variant_problems(seeds, steps: int, pool=None, per_cell: bool = False) -> list:
     """Problems of the inverted-F variant family (workloads.ifa_variant).
-    per_cell=False (FP32 material tables) carries the material grid only;
-    per_cell=True adds the 18 FP64 coefficient arrays the FP64 engine needs
-    (about 170 MB per variant, so build those a group at a time).  A process
+    per_cell=False carries the material grid only (about 0.7 MB): FP32-table
+    and FP64 engines build their coefficients from it on the device.
+    per_cell=True adds the 18 FP64 coefficient arrays built on the host
+    (about 170 MB per variant).  A process
     pool must make this package importable in its workers first (an
     initializer that loads it), or the workers cannot run the jobs."""
     jobs = [(int(s), steps, per_cell) for s in seeds]

@@ -87,16 +87,16 @@ def build_set(ES, pool, seeds, steps, policy, tiling):
     return np.array(x, np.float32), np.array(y, np.float32), keep, dev_s
 
 
-def plain_reference(ES, pool, seeds, policy, tiling, group=64):
+def plain_reference(ES, pool, seeds, policy, tiling, group=128):
     """S11 of plain FP64 batched runs of the full step count, and their wall
-    time (problem construction excluded).  The FP64 problems carry per-cell
-    coefficient arrays, so they are built one group at a time."""
+    time (problem construction excluded).  The FP64 engines build their
+    per-cell coefficients on the device from the material grids."""
     from special_topics_b200.backend import Batch, Engine
     freqs = ES.S11_FREQS
     seeds = list(seeds)
     ref, t_plain = [], 0.0
     for g0 in range(0, len(seeds), group):
-        probs = ES.variant_problems(seeds[g0:g0 + group], policy.n_total, pool, per_cell=True)
+        probs = ES.variant_problems(seeds[g0:g0 + group], policy.n_total, pool)
         engs = [Engine(p, "f64") for p in probs]
         try:
             t0 = time.perf_counter()
