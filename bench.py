@@ -30,7 +30,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "Gcell-updates/s & time-to-S11 at 0.1 dB: FP32/learned vs FP64 plain, 1 B200"
 FALLBACK_HBM_GBS = 6650.0
-NOMINAL_HBM_GBS = 8000.0   # the B200 HBM3e figure the north_star quotes
+NOMINAL_HBM_GBS = 8000.0   # nominal B200 HBM3e bandwidth (DGX figure)
 
 
 def _package():

@@ -204,7 +204,7 @@ int fdtd_status(fdtd_ctx* ctx, int* code, int* step);
 
 /* ---- batches: many handles advanced together (no counterpart in the reference,
  * which runs one problem per process through its global context,
- * fdtd_cuda.cu:44-118; the batched sweep is SURVEY's configuration 3) ---- */
+ * fdtd_cuda.cu:44-118; used for sweeps over antenna variants) ---- */
 typedef struct fdtd_batch fdtd_batch;
 
 /* Groups `count` handles of one device and one precision.  The batch owns no
@@ -261,9 +261,9 @@ int fdtd_ctx_read_farfield(fdtd_ctx* ctx, int array, double* re, double* im, lon
  * Results match the per-step form to FP32 rounding. */
 int fdtd_ctx_set_dft_block(fdtd_ctx* ctx, int steps);
 
-/* Checkpoint / restore (SURVEY's fdtd_save_state / load_state; the reference
- * has none): the evolving state of a handle -- fields, Psi, port traces,
- * far-field accumulators, watchdog and step -- to and from a caller buffer
+/* Checkpoint / restore (the reference has none): the evolving state of a
+ * handle -- fields, Psi, port traces, far-field accumulators, watchdog and
+ * step -- to and from a caller buffer
  * of fdtd_ctx_state_size bytes.  A state loads only into a handle set up
  * with the same problem (shape, precision, faces, probes, far field);
  * stepping on from a loaded state gives the results of stepping on from the

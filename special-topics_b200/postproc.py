@@ -184,8 +184,8 @@ def farfield_cuts(acc: dict, g: Grid, ff: FarFieldBox) -> list:
 def growth_onset(x, window: int = 250, factor: float = 10.0) -> int:
     """First step at which the envelope of a port trace (max |x| over windows
     of `window` steps) exceeds `factor` times its smallest value after the
-    pulse peak: where a run's late-time growth sets in (SURVEY 8(c)'s
-    stability check).  -1 when it never does."""
+    pulse peak: where a run's late-time growth sets in (a stability
+    check of long runs).  -1 when it never does."""
     x = np.abs(np.asarray(x, dtype=np.float64))
     nw = x.size // window
     if nw < 3:
