@@ -186,6 +186,9 @@ def main():
     ap.add_argument("--max-resid", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cache", default=None, help="npz of a previous run's training set and test reference")
+    ap.add_argument("--save-test-traces", action="store_true",
+                    help="also write the held-out runs' FP32 traces (es_test_traces.npz, about 110 KB per run) "
+                         "for replaying stop rules offline")
     ap.add_argument("--shape", default="16,4,1,0,0",
                     help="batch launch shape chunk,rows,prefetch,group,streams (backend.Batch.set_tiling)")
     args = ap.parse_args()
@@ -242,7 +245,8 @@ def main():
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
     metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling,
-                                     traces_out=os.path.join(args.out, "es_test_traces.npz"))
+                                     traces_out=os.path.join(args.out, "es_test_traces.npz")
+                                     if args.save_test_traces else None)
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
     print(json.dumps(metrics["evaluation"]), flush=True)
