@@ -193,12 +193,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
-    ap.add_argument("--tiling", default=None, help="fixed launch shape chunk,rows,prefetch (skips the tuner)")
+    ap.add_argument("--tiling", default=None, help="fixed launch shape chunk,rows,prefetch[,width] (skips the tuner)")
     ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
     ap.add_argument("--batch-tiling", default=None,
-                    help="fixed batch shape chunk,rows,prefetch,group[,streams] (skips the tuner)")
+                    help="fixed batch shape chunk,rows,prefetch,group[,streams[,width]] (skips the tuner)")
     ap.add_argument("--ttS11-members", dest="ttS11_members", type=int, default=64,
                     help="held-out variants of the time-to-S11 leg (0: skip)")
     args = ap.parse_args()
@@ -274,8 +274,9 @@ def main():
     from special_topics_b200 import autotune
     tuning = None
     if args.tiling:
-        ch, rw, pf = (int(x) for x in args.tiling.split(","))
-        tuning = {"chunk": ch, "rows": rw, "prefetch": pf, "ms_per_step": None}
+        v = [int(x) for x in args.tiling.split(",")]
+        tuning = {"chunk": v[0], "rows": v[1], "prefetch": v[2], "width": v[3] if len(v) > 3 else 32,
+                  "ms_per_step": None}
     elif not args.no_tune:
         scratch = build_problem_from_scenario(workloads.scaling_box(n, seed=1 + rank, steps=3000, ncpml=args.ncpml), 3000,
                                               per_cell=(args.precision != "f32-table"))
@@ -289,7 +290,7 @@ def main():
     if not args.no_e2e:
         eng = Engine(prob, args.precision, device=local)
         if tuning:
-            autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
+            autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
         h2d = _uploaded_bytes(prob, args.precision)
         eng.run(K)
         V, I = eng.voltages(K), eng.currents(K)
@@ -306,7 +307,7 @@ def main():
     # --- device-timed run
     eng = Engine(prob, args.precision, device=local)
     if tuning:
-        autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
+        autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
     eng.run(W)
     barrier()
     with ClockSampler(local) as clk:
@@ -336,7 +337,8 @@ def main():
                      "algorithmic_bytes_per_launch": byts[dom], "launch_ms": kern[dom],
                      "traffic": traffic},
         "kernel_ms": kern,
-        "tiling": {k: tuning[k] for k in ("chunk", "rows", "prefetch", "ms_per_step")} if tuning else "default",
+        "tiling": {k: tuning.get(k, 32 if k == "width" else None) for k in ("chunk", "rows", "prefetch", "width", "ms_per_step")}
+                  if tuning else "default",
         "clocks": clk.summary(),
         "gpu_launches": 4 * K,
         "e2e": e2e,
@@ -424,7 +426,8 @@ def _best_by_mode(table: list) -> dict:
         rows = [r for r in table if pick(r)]
         if rows:
             b = min(rows, key=lambda r: r["ms_per_step"])
-            out[name] = {k: b[k] for k in ("ms_per_step", "chunk", "rows", "prefetch", "group", "streams") if k in b}
+            out[name] = {k: b[k] for k in ("ms_per_step", "chunk", "rows", "prefetch", "group", "streams", "width")
+                         if k in b}
     return out
 
 
@@ -444,7 +447,7 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
         with Batch(engs) as b:
             if fixed:
                 v = [int(x) for x in fixed.split(",")]
-                b.set_tiling(v[0], v[1], v[2], v[3], v[4] if len(v) > 4 else 0)
+                b.set_tiling(v[0], v[1], v[2], v[3], v[4] if len(v) > 4 else 0, v[5] if len(v) > 5 else 32)
                 tuning = {"ms_per_step": None}
             else:
                 tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
@@ -560,7 +563,7 @@ def fp64_side(pkg, n=(256, 256, 256), K: int = 300, W: int = 8) -> dict:
     p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=1000), 1000)
     tuning = autotune.tune(p, "f64", steps_per_candidate=8)
     eng = Engine(p, "f64")
-    autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1))
+    autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
     eng.run(W)
     ms = eng.run_timed(K)
     kern = eng.profile_kernels(8)

@@ -183,11 +183,16 @@ int fdtd_ctx_read_material(fdtd_ctx* ctx, int comp, unsigned char* ids, long n, 
  * the end and returns FDTD_ERR_NONFINITE if a port sample went non-finite. */
 int fdtd_ctx_run(fdtd_ctx* ctx, int count);
 /* Launch shape of the two step kernels: each thread walks `x_planes_per_thread`
- * consecutive x planes of one (j, k) column; a block is 32 columns along k by
- * `block_rows` (1, 2, 4 or 8) along j.  Any shape gives the same results; the
+ * consecutive x planes of one (j, k) column; a block is `width` columns along k
+ * (fdtd_ctx_set_block_width: 32, the default, or 16, when a warp spans two
+ * rows, which wastes fewer lanes when nz + 1 is not a multiple of 32) by
+ * `block_rows` (1, 2, 4, 8 or 16) along j, in whole warps of at most 256
+ * threads (checked at the next run).  Any shape gives the same results; the
  * autotuner (special-topics_b200/autotune.py) picks the fastest per grid. */
 int fdtd_ctx_set_tiling(fdtd_ctx* ctx, int x_planes_per_thread, int block_rows);
 int fdtd_ctx_get_tiling(const fdtd_ctx* ctx, int* x_planes_per_thread, int* block_rows);
+int fdtd_ctx_set_block_width(fdtd_ctx* ctx, int threads_along_k);
+int fdtd_ctx_get_block_width(const fdtd_ctx* ctx, int* threads_along_k);
 /* How many x planes ahead the interior loop of the step kernels loads (1 or 2);
  * same results either way, chosen by the autotuner. */
 int fdtd_ctx_set_prefetch(fdtd_ctx* ctx, int planes);
@@ -231,6 +236,10 @@ int fdtd_batch_get_tiling(const fdtd_batch* batch, int* x_planes_per_thread, int
  * from one step to the next).  streams = 0 (default) is the tile-list mode.
  * Results are identical in both modes.  S <= 32. */
 int fdtd_batch_set_streams(fdtd_batch* batch, int streams);
+/* Block width along k of the batch's step launches (16 or 32), as
+ * fdtd_ctx_set_block_width. */
+int fdtd_batch_set_block_width(fdtd_batch* batch, int threads_along_k);
+int fdtd_batch_get_block_width(const fdtd_batch* batch, int* threads_along_k);
 int fdtd_batch_get_streams(const fdtd_batch* batch, int* streams);
 /* Runs `count` steps of every member.  All members must be at the same step and
  * have `count` steps left.  Returns FDTD_ERR_NONFINITE naming the first member

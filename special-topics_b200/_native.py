@@ -41,6 +41,8 @@ EXPORTS = (
     "fdtd_es_member_inputs", "fdtd_es_predict_members", "fdtd_ctx_farfield_post",
     "fdtd_ctx_set_dft_accumulator", "fdtd_ctx_state_size", "fdtd_ctx_save_state", "fdtd_ctx_load_state",
     "fdtd_ctx_set_dft_block", "fdtd_batch_set_streams", "fdtd_batch_get_streams",
+    "fdtd_ctx_set_block_width", "fdtd_ctx_get_block_width", "fdtd_batch_set_block_width",
+    "fdtd_batch_get_block_width",
 )
 
 
@@ -144,6 +146,10 @@ def lib() -> C.CDLL:
     L.fdtd_batch_get_tiling.argtypes = [v, ip, ip, ip, ip]
     L.fdtd_batch_set_streams.argtypes = [v, i]
     L.fdtd_batch_get_streams.argtypes = [v, ip]
+    L.fdtd_ctx_set_block_width.argtypes = [v, i]
+    L.fdtd_ctx_get_block_width.argtypes = [v, ip]
+    L.fdtd_batch_set_block_width.argtypes = [v, i]
+    L.fdtd_batch_get_block_width.argtypes = [v, ip]
     L.fdtd_batch_run.argtypes = [v, i]
     L.fdtd_batch_run_timed.argtypes = [v, i, fp]
     L.fdtd_batch_profile_kernels.argtypes = [v, i, dp]

@@ -44,9 +44,15 @@ def get_tiling(engine) -> tuple[int, int]:
     return a.value, b.value
 
 
-def set_tiling(engine, chunk: int, rows: int, prefetch: int = 1) -> None:
+def set_tiling(engine, chunk: int, rows: int, prefetch: int = 1, width: int = 32) -> None:
     N.check(N.lib().fdtd_ctx_set_tiling(engine._h, int(chunk), int(rows)))
     N.check(N.lib().fdtd_ctx_set_prefetch(engine._h, int(prefetch)))
+    N.check(N.lib().fdtd_ctx_set_block_width(engine._h, int(width)))
+
+
+# 16-wide blocks (a warp spans two rows) are tried at the best 32-wide
+# (chunk, prefetch) with these row counts
+NARROW_ROWS = (2, 4, 8, 16)
 
 
 def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64, use_cache: bool = True) -> dict:
@@ -57,7 +63,7 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
     if use_cache and key in cache:
         return cache[key]
     depths = prefetch_depths(precision)
-    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS) * len(depths)) + 8
+    need = 2 * steps_per_candidate * (len(CHUNKS) * len(ROWS) * len(depths) + len(NARROW_ROWS)) + 8
     if problem.grid.numberOfTimeSteps < need:
         raise ValueError(f"the scratch problem needs at least {need} time steps for tuning")
     nx = problem.grid.nx
@@ -72,9 +78,16 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
                     set_tiling(eng, chunk, rows, pf)
                     eng.run_timed(steps_per_candidate)          # capture and warm the graph
                     ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
-                    table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "ms_per_step": ms})
+                    table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "width": 32, "ms_per_step": ms})
+        best = min(table, key=lambda r: r["ms_per_step"])
+        for rows in NARROW_ROWS:
+            set_tiling(eng, best["chunk"], rows, best["prefetch"], 16)
+            eng.run_timed(steps_per_candidate)
+            ms = eng.run_timed(steps_per_candidate) / steps_per_candidate
+            table.append({"chunk": best["chunk"], "rows": rows, "prefetch": best["prefetch"], "width": 16,
+                          "ms_per_step": ms})
     best = min(table, key=lambda r: r["ms_per_step"])
-    out = {"chunk": best["chunk"], "rows": best["rows"], "prefetch": best["prefetch"],
+    out = {"chunk": best["chunk"], "rows": best["rows"], "prefetch": best["prefetch"], "width": best["width"],
            "ms_per_step": best["ms_per_step"], "table": table}
     cache[key] = out
     os.makedirs(os.path.dirname(CACHE), exist_ok=True)
@@ -104,7 +117,7 @@ def batch_steps_needed(steps_per_candidate: int, precision: str = "f32-table") -
     tile_mode = 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(prefetch_depths(precision))
                                            + len(BATCH_GROUPS))
     member_mode = 2 * MEMBER_STEPS * (len(BATCH_STREAMS) + len(MEMBER_SHAPES))
-    return tile_mode + member_mode
+    return tile_mode + 2 * steps_per_candidate * len(NARROW_ROWS) + member_mode
 
 
 def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> dict:
@@ -120,25 +133,28 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
     cache = _load()
     if use_cache and key in cache:
         r = cache[key]
-        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"], r.get("streams", 0))
+        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"], r.get("streams", 0), r.get("width", 32))
         return r
     max_x = max(e.problem.grid.nx for e in batch.engines) + 1
     table = []
 
-    def trial(chunk, rows, pf, group, streams=0, steps=steps_per_candidate):
-        batch.set_tiling(chunk, rows, pf, group, streams)
+    def trial(chunk, rows, pf, group, streams=0, steps=steps_per_candidate, width=32):
+        batch.set_tiling(chunk, rows, pf, group, streams, width)
         batch.run_timed(steps)              # capture and warm the graph
         ms = batch.run_timed(steps) / steps
         table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams,
-                      "ms_per_step": ms})
+                      "width": width, "ms_per_step": ms})
 
     for chunk in BATCH_CHUNKS:
         for rows in ROWS:
             for pf in prefetch_depths(batch.engines[0].precision):
                 trial(min(chunk, max_x), rows, pf, 0)
     best = min(table, key=lambda r: r["ms_per_step"])
+    for rows in NARROW_ROWS:
+        trial(best["chunk"], rows, best["prefetch"], 0, width=16)
+    best = min(table, key=lambda r: r["ms_per_step"])
     for group in BATCH_GROUPS[1:]:
-        trial(best["chunk"], best["rows"], best["prefetch"], group)
+        trial(best["chunk"], best["rows"], best["prefetch"], group, width=best["width"])
     ch, rw, pf = MEMBER_SHAPES[0]
     for streams in BATCH_STREAMS:
         trial(min(ch, max_x), rw, pf, 0, streams, MEMBER_STEPS)
@@ -147,7 +163,7 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
         trial(min(ch, max_x), rw, pf, 0, s_best, MEMBER_STEPS)
     best = min(table, key=lambda r: r["ms_per_step"])
     out = dict(best, table=table)
-    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"], best["streams"])
+    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"], best["streams"], best["width"])
     cache[key] = out
     os.makedirs(os.path.dirname(CACHE), exist_ok=True)
     with open(CACHE, "w") as f:
@@ -159,5 +175,5 @@ def apply(engine, precision: str, device: int = 0, scratch_problem=None) -> dict
     """Tunes (on scratch_problem, or the engine's own problem rebuilt with enough
     steps by the caller) and sets the best shape on `engine`."""
     res = tune(scratch_problem or engine.problem, precision, device)
-    set_tiling(engine, res["chunk"], res["rows"], res.get("prefetch", 1))
+    set_tiling(engine, res["chunk"], res["rows"], res.get("prefetch", 1), res.get("width", 32))
     return res

@@ -263,23 +263,29 @@ class Batch:
         self._h = h
         self.set_tiling(chunk, rows, prefetch, group, streams)
 
-    def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0, streams: int | None = None) -> None:
+    def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0, streams: int | None = None,
+                   width: int | None = None) -> None:
         """Launch shape (see fdtd_batch_set_tiling) and, when given, the
-        member-kernel worker stream count (fdtd_batch_set_streams)."""
+        member-kernel worker stream count (fdtd_batch_set_streams) and the
+        block width along k (fdtd_batch_set_block_width)."""
         N.check(N.lib().fdtd_batch_set_tiling(self._h, int(chunk), int(rows), int(prefetch), int(group)))
         if streams is not None:
             N.check(N.lib().fdtd_batch_set_streams(self._h, int(streams)))
+        if width is not None:
+            N.check(N.lib().fdtd_batch_set_block_width(self._h, int(width)))
 
     def set_shape(self, shape: dict) -> None:
-        """set_tiling from a dict as tiling() returns it ("streams" optional)."""
+        """set_tiling from a dict as tiling() returns it ("streams" and
+        "width" optional)."""
         self.set_tiling(shape["chunk"], shape["rows"], shape.get("prefetch", 1), shape.get("group", 0),
-                        shape.get("streams", 0))
+                        shape.get("streams", 0), shape.get("width", 32))
 
     def tiling(self) -> dict:
-        v = [C.c_int() for _ in range(5)]
+        v = [C.c_int() for _ in range(6)]
         N.check(N.lib().fdtd_batch_get_tiling(self._h, *[C.byref(x) for x in v[:4]]))
         N.check(N.lib().fdtd_batch_get_streams(self._h, C.byref(v[4])))
-        return dict(zip(("chunk", "rows", "prefetch", "group", "streams"), [x.value for x in v]))
+        N.check(N.lib().fdtd_batch_get_block_width(self._h, C.byref(v[5])))
+        return dict(zip(("chunk", "rows", "prefetch", "group", "streams", "width"), [x.value for x in v]))
 
     @property
     def cells(self) -> int:

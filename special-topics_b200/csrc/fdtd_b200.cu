@@ -125,6 +125,7 @@ struct fdtd_ctx {
   int* d_status = nullptr;
   // launch shape of the step kernels: x planes per thread, thread rows per block
   int ichunk = 1, block_rows = 8, prefetch = 1;
+  int block_w = 32;   // threads of a block along k (32: a warp is one row; 16: a warp spans two rows)
   // graph cache
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -408,6 +409,15 @@ struct KernelTimer {
   double ms[4] = {0, 0, 0, 0};
 };
 
+// A launch shape is whole warps of at most 256 threads (the step kernels'
+// launch bounds).
+int check_block(int w, int rows) {
+  const int t = w * rows;
+  if ((w != 16 && w != 32) || t > 256 || t % 32 != 0)
+    return fail(FDTD_ERR_BADARG, "block of %d x %d threads: need width 16 or 32, whole warps, at most 256", w, rows);
+  return FDTD_OK;
+}
+
 // Enqueue `count` steps on stream `st` (default: the handle's stream; with
 // `tm`, one step at a time, timing each kernel).
 template <typename T, class C, bool EXACT>
@@ -417,8 +427,10 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   Probes pr = dev_probes(c);
   FarField ff = dev_ff(c);
   // a thread per (j, k) column walks `ichunk` x planes
-  const dim3 blk(32, c->block_rows);
-  const dim3 grd((c->nz + 1 + 31) / 32, (c->ny + c->block_rows) / c->block_rows,
+  int rc0 = check_block(c->block_w, c->block_rows);
+  if (rc0) return rc0;
+  const dim3 blk(c->block_w, c->block_rows);
+  const dim3 grd((c->nz + c->block_w) / c->block_w, (c->ny + c->block_rows) / c->block_rows,
                  (c->nx + 1 + c->ichunk - 1) / c->ichunk);
   const long long plane = (long long)c->ny * (c->nz + 1);
   const unsigned mid_blocks = (unsigned)((plane + pr.n_i + 255) / 256);
@@ -428,8 +440,8 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   auto kh = step_kernel<T, C, EXACT>(false, c->prefetch);
   auto ke = step_kernel<T, C, EXACT>(true, c->prefetch);
   size_t smem = 0;
-  int rc = stage_smem(kh, c->prefetch, 32 * c->block_rows, &smem);
-  if (!rc) rc = stage_smem(ke, c->prefetch, 32 * c->block_rows, &smem);
+  int rc = stage_smem(kh, c->prefetch, c->block_w * c->block_rows, &smem);
+  if (!rc) rc = stage_smem(ke, c->prefetch, c->block_w * c->block_rows, &smem);
   if (rc) return rc;
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], st));
@@ -535,6 +547,7 @@ int close_dft_block(fdtd_ctx* c, int upto, cudaStream_t st) {
 }
 
 constexpr int kGraphSteps = 64;
+
 constexpr int kMaxBatchStreams = 32;
 
 int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* tm = nullptr) {
@@ -1240,11 +1253,26 @@ int fdtd_ctx_set_tiling(fdtd_ctx* c, int x_planes_per_thread, int block_rows) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
   if (x_planes_per_thread < 1 || x_planes_per_thread > c->nx + 1)
     return fail(FDTD_ERR_BADARG, "x planes per thread %d not in 1..%d", x_planes_per_thread, c->nx + 1);
-  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8)
-    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8}", block_rows);
+  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8 && block_rows != 16)
+    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8,16}", block_rows);
   c->ichunk = x_planes_per_thread;
   c->block_rows = block_rows;
   invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_set_block_width(fdtd_ctx* c, int threads_along_k) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (threads_along_k != 16 && threads_along_k != 32)
+    return fail(FDTD_ERR_BADARG, "block width %d not 16 or 32", threads_along_k);
+  c->block_w = threads_along_k;
+  invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_get_block_width(const fdtd_ctx* c, int* threads_along_k) {
+  if (!c || !threads_along_k) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *threads_along_k = c->block_w;
   return FDTD_OK;
 }
 
@@ -1658,6 +1686,7 @@ struct fdtd_batch {
   int prec = FDTD_PREC_F32_TABLE;
   std::vector<fdtd_ctx*> m;
   int ichunk = 8, block_rows = 4, prefetch = 1, group = 0;
+  int block_w = 32;
   void* d_inst = nullptr;
   size_t inst_size = 0;  // bytes of one Instance
   BatchTile* d_tiles = nullptr;
@@ -1730,7 +1759,7 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
     in.pr = dev_probes(c);
     in.ff = dev_ff(c);
     memcpy(host.data() + (size_t)q * sizeof(In), &in, sizeof(In));
-    const int gx = (c->nz + 1 + 31) / 32, gy = (c->ny + b->block_rows) / b->block_rows,
+    const int gx = (c->nz + b->block_w) / b->block_w, gy = (c->ny + b->block_rows) / b->block_rows,
               gz = (c->nx + 1 + b->ichunk - 1) / b->ichunk;
     if (gx > 65535 || gy > 65535 || gz > 65535)
       return fail(FDTD_ERR_BADARG, "batch member %d: %dx%dx%d tiles exceed the tile index range", q, gx, gy, gz);
@@ -1774,7 +1803,9 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
   // persistent grids: as many blocks as fit on the device at once
   int sms = 0, per_h = 0, per_e = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-  const int threads = 32 * b->block_rows;
+  int rc0 = check_block(b->block_w, b->block_rows);
+  if (rc0) return rc0;
+  const int threads = b->block_w * b->block_rows;
   size_t smem = 0;
   auto kh = batch_kernel<T, C, EXACT>(false, b->prefetch, true);
   auto ke = batch_kernel<T, C, EXACT>(true, b->prefetch, true);
@@ -1792,14 +1823,14 @@ template <typename T, class C, bool EXACT>
 int batch_enqueue(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
   const Instance<T, C>* in = (const Instance<T, C>*)b->d_inst;
   const int nt = (int)b->tiles.size();
-  const dim3 blk(32, b->block_rows);
+  const dim3 blk(b->block_w, b->block_rows);
   const unsigned gh = b->group ? (unsigned)std::min(b->grid_h, (nt + b->group - 1) / b->group) : (unsigned)nt;
   const unsigned ge = b->group ? (unsigned)std::min(b->grid_e, (nt + b->group - 1) / b->group) : (unsigned)nt;
   auto kh = batch_kernel<T, C, EXACT>(false, b->prefetch, b->group != 0);
   auto ke = batch_kernel<T, C, EXACT>(true, b->prefetch, b->group != 0);
   size_t smem = 0;
-  int rc = stage_smem(kh, b->prefetch, 32 * b->block_rows, &smem);
-  if (!rc) rc = stage_smem(ke, b->prefetch, 32 * b->block_rows, &smem);
+  int rc = stage_smem(kh, b->prefetch, b->block_w * b->block_rows, &smem);
+  if (!rc) rc = stage_smem(ke, b->prefetch, b->block_w * b->block_rows, &smem);
   if (rc) return rc;
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], b->stream));
@@ -1866,16 +1897,19 @@ int batch_enqueue_any(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
 // duration of a scope (its own shape comes back afterwards).
 struct MemberShape {
   fdtd_ctx* c;
-  int ichunk, rows, pf;
-  MemberShape(fdtd_ctx* m, const fdtd_batch* b) : c(m), ichunk(m->ichunk), rows(m->block_rows), pf(m->prefetch) {
+  int ichunk, rows, pf, w;
+  MemberShape(fdtd_ctx* m, const fdtd_batch* b)
+      : c(m), ichunk(m->ichunk), rows(m->block_rows), pf(m->prefetch), w(m->block_w) {
     m->ichunk = b->ichunk;
     m->block_rows = b->block_rows;
     m->prefetch = b->prefetch;
+    m->block_w = b->block_w;
   }
   ~MemberShape() {
     c->ichunk = ichunk;
     c->block_rows = rows;
     c->prefetch = pf;
+    c->block_w = w;
   }
 };
 
@@ -2113,8 +2147,8 @@ int fdtd_batch_set_tiling(fdtd_batch* b, int x_planes_per_thread, int block_rows
   if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
   if (x_planes_per_thread < 1 || x_planes_per_thread > 1024)
     return fail(FDTD_ERR_BADARG, "x planes per thread %d outside 1..1024", x_planes_per_thread);
-  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8)
-    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8}", block_rows);
+  if (block_rows != 1 && block_rows != 2 && block_rows != 4 && block_rows != 8 && block_rows != 16)
+    return fail(FDTD_ERR_BADARG, "block rows %d not in {1,2,4,8,16}", block_rows);
   if (prefetch < 1 || prefetch > 4) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in 1..4", prefetch);
   if (prefetch > 2 && b->prec != FDTD_PREC_F32_TABLE)
     return fail(FDTD_ERR_BADARG, "prefetch depths 3 and 4 (shared-memory stages) need material-table members");
@@ -2126,6 +2160,21 @@ int fdtd_batch_set_tiling(fdtd_batch* b, int x_planes_per_thread, int block_rows
   b->block_rows = block_rows;
   b->prefetch = prefetch;
   b->group = group;
+  return FDTD_OK;
+}
+
+int fdtd_batch_set_block_width(fdtd_batch* b, int threads_along_k) {
+  if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
+  if (threads_along_k != 16 && threads_along_k != 32)
+    return fail(FDTD_ERR_BADARG, "block width %d not 16 or 32", threads_along_k);
+  if (threads_along_k != b->block_w) batch_drop_graph(b);
+  b->block_w = threads_along_k;
+  return FDTD_OK;
+}
+
+int fdtd_batch_get_block_width(const fdtd_batch* b, int* threads_along_k) {
+  if (!b || !threads_along_k) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *threads_along_k = b->block_w;
   return FDTD_OK;
 }
 

@@ -766,7 +766,7 @@ __device__ __forceinline__ void h_tile_planes(const StepParams<T, C>& p, const H
   h_band_range<T, C, EXACT, BPF, kFX | YZ>(p, c, cb, xb, i1, ez_c, ey_c);
 }
 
-// H update of one tile: columns (bx*32 + tx, by*rows + ty), x planes from
+// H update of one tile: columns (bx*width + tx, by*rows + ty), x planes from
 // bz*ichunk.  PF: how many planes ahead the interior loop loads.
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, int by, int bz) {
@@ -787,8 +787,8 @@ __device__ __forceinline__ void step_h_tile(const StepParams<T, C>& p, int bx, i
   c.yp = band_ci(p.face[3], j, false);
   c.zn = band_ci(p.face[4], k, false);
   c.zp = band_ci(p.face[5], k, false);
-  // a warp is 32 consecutive k of one j: y band membership is uniform over
-  // it, z band membership is per lane
+  // a warp is 32 consecutive k of one j (or, in 16-wide blocks, 16 k of two
+  // rows); band membership is tested per lane, the votes only pick the form
   const bool ycol = c.yn >= 0 || c.yp >= 0, zcol = c.zn >= 0 || c.zp >= 0;
   const bool warp_lean = __all_sync(0xffffffffu, !valid || (!ycol && !zcol));
   const bool warp_y = __any_sync(0xffffffffu, valid && ycol);

@@ -67,7 +67,8 @@ def test_batch_matches_solo_runs(solo, chunk, rows, pf, group, streams):
     engs = [Engine(p, precision) for p in _members()]
     try:
         with Batch(engs, chunk, rows, pf, group, streams) as b:
-            assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams}
+            assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams,
+                                  "width": 32}
             b.run(STEPS)
             assert b.step == STEPS
         for q, e in enumerate(engs):
@@ -271,3 +272,21 @@ def test_early_stop_driver_keeps_each_runs_own_traces():
             n = r["stopped_at"]
             assert np.array_equal(r["V"][:n], solo[q][0][:n])
             assert np.array_equal(r["I"][:n], solo[q][1][:n])
+
+
+@pytest.mark.parametrize("chunk,rows,pf,group,streams", [(8, 4, 1, 0, 0), (5, 16, 2, 3, 0), (16, 2, 1, 0, 2)])
+def test_batch_with_16_wide_blocks_matches_solo_runs(solo, chunk, rows, pf, group, streams):
+    """16-wide blocks (a warp spans two rows) in the tile-list, persistent and
+    member-kernel modes."""
+    precision, states = solo
+    engs = [Engine(p, precision) for p in _members()]
+    try:
+        with Batch(engs, chunk, rows, pf, group, streams) as b:
+            b.set_tiling(chunk, rows, pf, group, streams, 16)
+            assert b.tiling()["width"] == 16
+            b.run(STEPS)
+        for q, e in enumerate(engs):
+            _assert_same(states[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()

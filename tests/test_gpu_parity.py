@@ -217,15 +217,18 @@ def test_device_tables_run_matches_host_tables_run():
         assert np.array_equal(a.field("Ez"), b.field("Ez"))
 
 
-@pytest.mark.parametrize("chunk,rows,pf", [(1, 1, 1), (3, 2, 2), (7, 8, 1), (64, 4, 2), (2, 4, 2)])
-def test_launch_shape_does_not_change_fp64_results(chunk, rows, pf):
+@pytest.mark.parametrize("chunk,rows,pf,width", [(1, 1, 1, 32), (3, 2, 2, 32), (7, 8, 1, 32), (64, 4, 2, 32),
+                                                 (2, 4, 2, 32),
+                                                 # 16-wide blocks: a warp spans two rows
+                                                 (4, 2, 1, 16), (5, 16, 2, 16), (1, 8, 1, 16)])
+def test_launch_shape_does_not_change_fp64_results(chunk, rows, pf, width):
     from special_topics_b200 import autotune
     scn, steps = CASES["small-zp"]()
     o = oracle.Oracle(scn, steps)
     o.step(steps)
     p = build_problem_from_scenario(scn, steps)
     with Engine(p, "f64") as eng:
-        autotune.set_tiling(eng, min(chunk, p.grid.nx + 1), rows, pf)
+        autotune.set_tiling(eng, min(chunk, p.grid.nx + 1), rows, pf, width)
         eng.run(steps)
         assert np.array_equal(eng.voltages()[0], o.get("V:0"))
         for fld in ("Hx", "Ey", "Ez"):
@@ -236,7 +239,7 @@ def test_autotuner_picks_a_measured_shape(tmp_path, monkeypatch):
     from special_topics_b200 import autotune
     monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tiling.json"))
     scn, _ = CASES["small-xp"]()
-    p = build_problem_from_scenario(scn, 1400)
+    p = build_problem_from_scenario(scn, 1500)
     res = autotune.tune(p, "f32-table", steps_per_candidate=8)
     assert {"chunk", "rows", "ms_per_step"} <= set(res)
     assert res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
@@ -281,16 +284,18 @@ def test_kahan_fp32_accumulators_track_fp64_ones():
             N.check(N.lib().fdtd_ctx_set_dft_accumulator(c._h, 1))
 
 
-@pytest.mark.parametrize("chunk,rows,pf", [(5, 2, 3), (16, 8, 4), (1, 4, 4), (64, 2, 3), (3, 8, 2)])
-def test_shared_memory_stages_give_identical_table_results(chunk, rows, pf):
+@pytest.mark.parametrize("chunk,rows,pf,width", [(5, 2, 3, 32), (16, 8, 4, 32), (1, 4, 4, 32), (64, 2, 3, 32),
+                                                 (3, 8, 2, 32), (8, 4, 1, 16), (6, 16, 3, 16), (16, 2, 4, 16)])
+def test_shared_memory_stages_give_identical_table_results(chunk, rows, pf, width):
     """Prefetch depths 3 and 4 stage the interior planes through shared
-    memory; material-table results are bit-identical to the depth-1 form."""
+    memory; material-table results are bit-identical to the depth-1 form,
+    also with 16-wide blocks."""
     from special_topics_b200 import autotune
     scn, steps = CASES["ifa-fr4-substrate"]()
     p = build_problem_from_scenario(scn, steps, per_cell=False)
     with Engine(p, "f32-table") as a, Engine(p, "f32-table") as b:
         autotune.set_tiling(a, 8, 4, 1)
-        autotune.set_tiling(b, min(chunk, p.grid.nx + 1), rows, pf)
+        autotune.set_tiling(b, min(chunk, p.grid.nx + 1), rows, pf, width)
         a.run(steps)
         b.run(steps)
         assert np.array_equal(a.voltages()[0], b.voltages()[0])
@@ -354,3 +359,24 @@ def test_time_blocked_dft_matches_per_step(acc):
     with Engine(build_problem_from_scenario(scn, 200), "f64") as d:
         with pytest.raises(N.FdtdError):
             N.check(N.lib().fdtd_ctx_set_dft_block(d._h, 16))
+
+
+def test_block_width_validation():
+    from special_topics_b200 import autotune
+    scn, steps = CASES["small-xp"]()
+    p = build_problem_from_scenario(scn, steps, per_cell=False)
+    with Engine(p, "f32-table") as e:
+        with pytest.raises(N.FdtdError):
+            N.check(N.lib().fdtd_ctx_set_block_width(e._h, 8))
+        autotune.set_tiling(e, 4, 1, 1, 16)       # 16 threads: not a whole warp, refused at the run
+        with pytest.raises(N.FdtdError) as ei:
+            e.run(2)
+        assert ei.value.code == N.FDTD_ERR_BADARG
+        autotune.set_tiling(e, 4, 16, 1, 32)      # 512 threads: above the launch bounds
+        with pytest.raises(N.FdtdError):
+            e.run(2)
+        autotune.set_tiling(e, 4, 16, 1, 16)
+        e.run(2)
+        w = ctypes.c_int()
+        N.check(N.lib().fdtd_ctx_get_block_width(e._h, ctypes.byref(w)))
+        assert w.value == 16
