@@ -96,7 +96,7 @@ def tune(problem, precision: str, device: int = 0, steps_per_candidate: int = 64
     return out
 
 
-BATCH_CHUNKS = (2, 4, 8, 16, 32)
+BATCH_CHUNKS = (2, 4, 8, 16, 32, 64)   # 64 is cut to the members' depth: one x chunk per column
 BATCH_GROUPS = (0, 1, 2, 4, 8, 16)
 # member-kernel mode: worker stream counts and member launch shapes tried
 BATCH_STREAMS = (2, 3, 4, 6, 8, 16)
