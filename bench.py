@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--tiling", default=None, help="fixed launch shape chunk,rows,prefetch[,width] (skips the tuner)")
     ap.add_argument("--tune-steps", type=int, default=16, help="steps timed per autotuner candidate")
+    ap.add_argument("--dft-block", type=int, default=16,
+                    help="FP32 legs: time-blocked far-field DFT, steps per block (0: accumulate every step)")
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
     ap.add_argument("--batch-tiling", default=None,
@@ -264,6 +266,7 @@ def main():
             variants = variant_problems(seeds, max(7000, vsteps), pool)
 
     K, W, P = args.steps, args.warmup, 16
+    dft_block = args.dft_block if args.precision != "f64" else 0   # FP64 keeps the reference's per-step sums
     scn = workloads.scaling_box(n, seed=1 + rank, steps=K + W + P, ncpml=args.ncpml)
     t0 = time.perf_counter()
     prob = build_problem_from_scenario(scn, K + W + P, per_cell=(args.precision != "f32-table"))
@@ -288,7 +291,7 @@ def main():
     e2e = None
     t0 = time.perf_counter()
     if not args.no_e2e:
-        eng = Engine(prob, args.precision, device=local)
+        eng = Engine(prob, args.precision, device=local, dft_block=dft_block)
         if tuning:
             autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
         h2d = _uploaded_bytes(prob, args.precision)
@@ -305,7 +308,7 @@ def main():
                        "K steps, readback of port traces and far-field accumulators"}
 
     # --- device-timed run
-    eng = Engine(prob, args.precision, device=local)
+    eng = Engine(prob, args.precision, device=local, dft_block=dft_block)
     if tuning:
         autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
     eng.run(W)
@@ -329,6 +332,7 @@ def main():
         "data": "synthetic (seeded scaling-box scenario in the reference's JSON schema)",
         "config": {"workload": workload, "cells": cells, "precision": args.precision,
                    "time_steps_in_problem": K + W + P, "far_field_freqs": 2,
+                   "far_field_dft": f"time-blocked, {dft_block} steps per block" if dft_block else "every step",
                    "l2": "inputs larger than L2 (fields and ids >> 126 MB), no flush needed",
                    "parallelism": f"{world} independent problem(s), one per GPU"},
         "roofline": {"bound": "hbm", "kernel": f"k_step_{dom}", "achieved": achieved, "peak": peak,
@@ -340,13 +344,14 @@ def main():
         "tiling": {k: tuning.get(k, 32 if k == "width" else None) for k in ("chunk", "rows", "prefetch", "width", "ms_per_step")}
                   if tuning else "default",
         "clocks": clk.summary(),
-        "gpu_launches": 4 * K,
+        "gpu_launches": (5 if dft_block else 4) * K,   # H, mid, E, epilogue (+ the DFT flush)
         "e2e": e2e,
         "setup_s": setup_s,
     }
     if variants is not None:
         if variants:
             bs = batched_side(variants, K=args.batch_steps, W=args.warmup, tune_steps=args.tune_steps,
+                              dft_block=args.dft_block,
                               device=local, barrier=barrier, fixed=args.batch_tiling)
         else:                       # a rank with no members still takes the same collective steps
             bs = None
@@ -364,7 +369,7 @@ def main():
             line["batched"] = bs
     if rank == 0 and world == 1 and args.ttS11_members > 0:
         try:
-            line["time_to_s11"] = time_to_s11_side(args.ttS11_members, device=local)
+            line["time_to_s11"] = time_to_s11_side(args.ttS11_members, device=local, dft_block=args.dft_block)
         except Exception as e:  # this leg must not hide the main number
             line["time_to_s11"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_fp64:
@@ -432,7 +437,7 @@ def _best_by_mode(table: list) -> dict:
 
 
 def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, device: int = 0,
-                 barrier=lambda: None, fixed: str | None = None) -> dict:
+                 barrier=lambda: None, fixed: str | None = None, dft_block: int = 0) -> dict:
     """The batched sweep (FP32 fields, material tables): every member advanced
     either by one set of four launches per step for the whole batch (tile-list
     mode) or by its own four kernels per step on worker streams inside one
@@ -441,7 +446,7 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
     from special_topics_b200 import autotune
     from special_topics_b200.backend import Batch, Engine
     t0 = time.perf_counter()
-    engs = [Engine(p, "f32-table", device=device) for p in problems]
+    engs = [Engine(p, "f32-table", device=device, dft_block=dft_block) for p in problems]
     create_s = time.perf_counter() - t0
     try:
         with Batch(engs) as b:
@@ -482,10 +487,12 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
     ach = roof_bytes / (roof_ms / 1e3) / 1e9
     dims = [(p.grid.nx, p.grid.ny, p.grid.nz) for p in problems]
     return {"workload": f"ifa-variants-{len(problems)}", "members": len(problems), "cells": cells,
+            "far_field_dft": f"time-blocked, {dft_block} steps per block" if dft_block else "every step",
             "grid_min": list(min(dims, key=lambda d: d[0] * d[1] * d[2])),
             "grid_max": list(max(dims, key=lambda d: d[0] * d[1] * d[2])),
             "value": cells * K / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "steps": K, "warmup": W,
-            "ms_per_step": ms / K, "gpu_launches": 4 * K * (len(problems) if tiling.get("streams", 0) else 1),
+            "ms_per_step": ms / K,
+            "gpu_launches": (5 if dft_block else 4) * K * (len(problems) if tiling.get("streams", 0) else 1),
             "kernel_ms": kern,
             "tiling": tiling, "tuning_ms_per_step": tuning["ms_per_step"],
             "tuning_best_ms_by_mode": _best_by_mode(tuning.get("table", [])),
@@ -499,7 +506,7 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
 WEIGHTS = os.path.join(ROOT, "special-topics_b200", "weights", "es_ifa_variants.npz")
 
 
-def time_to_s11_side(count: int, device: int = 0) -> dict:
+def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     """Time-to-S11 on inverted-F variants that neither training (seeds 1000..)
     nor the choice of the stop rule's thresholds (seeds 10000..10255) saw
     (seeds 20000..): plain FP64
@@ -535,7 +542,7 @@ def time_to_s11_side(count: int, device: int = 0) -> dict:
         for e in engs:
             e.close()
     for name, use in (("learned", True), ("no_network", False)):
-        engs = [Engine(p, "f32-table", device=device) for p in probs]
+        engs = [Engine(p, "f32-table", device=device, dft_block=dft_block) for p in probs]
         try:
             t0 = time.perf_counter()
             res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use)
