@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in this folder from the reference checkout.
 
-Run in a container that has the reference mounted:
-    python tests/golden/make_golden.py [/path/to/reference]
+Run where a reference checkout is available, naming its root either as the
+argument or in the REFERENCE_ROOT environment variable:
+    python tests/golden/make_golden.py /path/to/reference
 
 It copies
   * js_fdtd/results/out.json -- the only reference-produced Float64 output: the
@@ -45,4 +46,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set REFERENCE_ROOT)")
+    main(root)
