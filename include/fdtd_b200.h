@@ -225,7 +225,10 @@ int fdtd_batch_size(const fdtd_batch* batch);
  * fdtd_ctx_set_tiling, prefetch depth as in fdtd_ctx_set_prefetch, and `group`:
  * 0 = one block per tile; g > 0 = a persistent grid (as many blocks as are
  * resident on the device) whose blocks claim g consecutive tiles at a time from
- * a device counter.  Results do not depend on the shape. */
+ * a device counter.  Results do not depend on the shape.  x_planes_per_thread
+ * may be 1..1024 whatever the members' depth: a member with nx + 1 planes or
+ * fewer than it gets one chunk per column, and fdtd_batch_get_tiling reports
+ * the value as set, not the per-member value in effect. */
 int fdtd_batch_set_tiling(fdtd_batch* batch, int x_planes_per_thread, int block_rows, int prefetch, int group);
 int fdtd_batch_get_tiling(const fdtd_batch* batch, int* x_planes_per_thread, int* block_rows, int* prefetch,
                           int* group);
@@ -272,10 +275,14 @@ int fdtd_ctx_set_dft_block(fdtd_ctx* ctx, int steps);
 
 /* Checkpoint / restore (the reference has none): the evolving state of a
  * handle -- fields, Psi, port traces, far-field accumulators, watchdog and
- * step -- to and from a caller buffer
- * of fdtd_ctx_state_size bytes.  A state loads only into a handle set up
- * with the same problem (shape, precision, faces, probes, far field);
- * stepping on from a loaded state gives the results of stepping on from the
+ * step -- to and from a caller buffer of fdtd_ctx_state_size bytes.  The
+ * state carries a 64-bit digest of everything the handle was set up with:
+ * grid, cell sizes, dt, step count, precision and the data of every set-up
+ * call (coefficients or material grid and tables, CPML profiles and CPsi,
+ * sources, probes, far-field frequencies and box), in call order.  A state
+ * loads only into a handle whose digest matches, that is one set up by the
+ * same calls with the same data; any other fails with FDTD_ERR_BADARG.
+ * Stepping on from a loaded state gives the results of stepping on from the
  * saved one. */
 int fdtd_ctx_state_size(fdtd_ctx* ctx, long long* bytes);
 int fdtd_ctx_save_state(fdtd_ctx* ctx, void* buf, long long bytes);
@@ -286,6 +293,22 @@ int fdtd_ctx_load_state(fdtd_ctx* ctx, const void* buf, long long bytes);
  * returns FP64 either way.  Set before the first step; FP64 problems keep
  * FP64.  No counterpart in the reference (its accumulators are Float64Array). */
 int fdtd_ctx_set_dft_accumulator(fdtd_ctx* ctx, int kahan_fp32);
+
+/* The E update at the x = max wall.  The reference's updateE runs Ey and Ez
+ * up to i = nx inclusive (js_fdtd/assembly/fdtd_kernels.ts:159,185 with the
+ * worker range end nxp1, js_fdtd/src/fdtdWorker.js:22-30) and there reads one
+ * plane past the Hz and Hy arrays, which in its shared memory are Ex(i=0) and
+ * the start of Hz: a coupling of the two x walls that grows without bound at
+ * late times (js_fdtd/scenarios/ifa-matlab-7000.json:3).  The MATLAB original
+ * updates Ey, Ez only for i < nx (fdtd_solve_Ch9_ex9a_12032026.m.txt:2095-2106),
+ * a PEC wall.
+ *   wall = 0: the reference's reads (default for FDTD_PREC_F64: bit parity);
+ *   wall = 1: Ey and Ez at i = nx are never updated and stay zero (default for
+ *             the FP32 precisions, whose rounding would otherwise seed the
+ *             growing mode some nine orders of magnitude above FP64's).
+ * May be changed between runs. */
+int fdtd_ctx_set_x_wall(fdtd_ctx* ctx, int wall);
+int fdtd_ctx_get_x_wall(const fdtd_ctx* ctx, int* wall);
 
 /* Far-field post-processing on the device from the handle's accumulators
  * (farfield.js:257-607): radp[f] = radiated power at frequency f, and the
@@ -308,7 +331,10 @@ int fdtd_dft(const double* x, int N, double dt, const double* freqs, int M, doub
  * the library holds until the process exits.  Limits: N <= 32768 samples and
  * M <= 4096 frequencies; larger calls fail with FDTD_ERR_BADARG.  The first
  * call on a device looks up that array's address, so make that first call
- * before any stream capture.  All calls share the array: calls that overlap on
+ * before any stream capture.  The address is kept for the life of the process:
+ * it assumes the device's primary context does too (a host that resets the
+ * device with cudaDeviceReset must not call this entry point afterwards).
+ * All calls share the array: calls that overlap on
  * the GPU (from several host threads) race and must be serialised by the
  * caller.  Each call writes every value it reads, so no call sees another's. */
 int fdtd_dft_noalloc(const double* x, int N, double dt, const double* freqs, int M, double shift, double* re,

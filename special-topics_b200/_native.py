@@ -42,7 +42,7 @@ EXPORTS = (
     "fdtd_ctx_set_dft_accumulator", "fdtd_ctx_state_size", "fdtd_ctx_save_state", "fdtd_ctx_load_state",
     "fdtd_ctx_set_dft_block", "fdtd_batch_set_streams", "fdtd_batch_get_streams",
     "fdtd_ctx_set_block_width", "fdtd_ctx_get_block_width", "fdtd_batch_set_block_width",
-    "fdtd_batch_get_block_width",
+    "fdtd_batch_get_block_width", "fdtd_ctx_set_x_wall", "fdtd_ctx_get_x_wall",
 )
 
 
@@ -134,6 +134,8 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_farfield_post.argtypes = [v, dp, dp, i, dp, dp, dp]
     L.fdtd_ctx_set_dft_accumulator.argtypes = [v, i]
     L.fdtd_ctx_set_dft_block.argtypes = [v, i]
+    L.fdtd_ctx_set_x_wall.argtypes = [v, i]
+    L.fdtd_ctx_get_x_wall.argtypes = [v, ip]
     L.fdtd_ctx_state_size.argtypes = [v, P(C.c_longlong)]
     L.fdtd_ctx_save_state.argtypes = [v, v, C.c_longlong]
     L.fdtd_ctx_load_state.argtypes = [v, v, C.c_longlong]

@@ -30,12 +30,15 @@ class Engine:
     """One problem resident on one GPU."""
 
     def __init__(self, problem: Problem, precision: str = "f64", device: int = 0, host_tables: bool = False,
-                 dft_accumulator: str = "f64", dft_block: int = 0):
+                 dft_accumulator: str = "f64", dft_block: int = 0, x_wall: bool | None = None):
         """host_tables=True builds an FP32-table problem's ids with numpy
         (tables.build_tables, needs per-cell material arrays) instead of on the
         device (fdtd_ctx_build_material).  dft_accumulator "kahan-f32" keeps an
         FP32 problem's far-field accumulators as compensated FP32 pairs; dft_block
-        > 0 accumulates the surface DFT once per that many steps (FP32)."""
+        > 0 accumulates the surface DFT once per that many steps (FP32).
+        x_wall: None keeps the precision's default (FP64: the reference's reads
+        past Hz/Hy at i = nx; FP32: Ey, Ez at i = nx held at zero), True / False
+        forces the wall / the reference's reads (fdtd_ctx_set_x_wall)."""
         if dft_accumulator not in ("f64", "kahan-f32"):
             raise ValueError("dft_accumulator must be 'f64' or 'kahan-f32'")
         if precision not in PRECISIONS:
@@ -56,6 +59,8 @@ class Engine:
                 N.check(L.fdtd_ctx_set_dft_accumulator(h, 1))
             if dft_block:
                 N.check(L.fdtd_ctx_set_dft_block(h, int(dft_block)))
+            if x_wall is not None:
+                N.check(L.fdtd_ctx_set_x_wall(h, int(bool(x_wall))))
         except Exception:
             self.close()
             raise
@@ -124,6 +129,16 @@ class Engine:
             fi = np.ascontiguousarray(vs.field_indices, dtype=np.int32)
             trip = np.ascontiguousarray(vs.override, dtype=np.float64).reshape(-1)
             N.check(L.fdtd_ctx_override_material(h, vs.axis, N.iptr(fi), N.dptr(trip), fi.size))
+
+    @property
+    def x_wall(self) -> bool:
+        w = C.c_int()
+        N.check(N.lib().fdtd_ctx_get_x_wall(self._h, C.byref(w)))
+        return bool(w.value)
+
+    @x_wall.setter
+    def x_wall(self, wall: bool) -> None:
+        N.check(N.lib().fdtd_ctx_set_x_wall(self._h, int(bool(wall))))
 
     def material(self, comp: str) -> tuple[np.ndarray, np.ndarray]:
         """(ids, FP64 table rows x 3) of a table problem's component."""

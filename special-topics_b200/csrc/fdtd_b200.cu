@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -116,6 +117,7 @@ struct fdtd_ctx {
   std::vector<double> ffreq;  // far-field frequencies (Hz)
   int acc_kahan = 0;          // FP32 problems: compensated FP32 accumulator pairs instead of FP64
   int dft_block = 0;          // FP32 problems: steps per time block of the surface DFT (0: every step)
+  int x_wall = 0;             // 1: Ey, Ez at i = nx stay zero (see fdtd_ctx_set_x_wall)
   float* dft_samples = nullptr;
   int* d_dft_done = nullptr;
   long long ffsz[3] = {};
@@ -131,6 +133,10 @@ struct fdtd_ctx {
   int graph_steps = 0;
   bool dirty = true;
   std::vector<void*> owned;  // every device allocation
+  // Running digest of everything the handle was set up with: shape, spacing,
+  // dt, step count, precision and the arguments of every upload call in call
+  // order.  A saved state carries it and loads only where it matches.
+  unsigned long long setup_digest = 0x6a09e667f3bcc908ULL;
 };
 
 namespace {
@@ -378,6 +384,7 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   p.bands_disjoint = bands_disjoint(c);
   p.dft_block = c->dft_block;
   p.dft_done = c->d_dft_done;
+  p.x_wall = c->x_wall;
   return p;
 }
 
@@ -619,6 +626,33 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
   return FDTD_OK;
 }
 
+unsigned long long mix64(unsigned long long h, unsigned long long w) {
+  h ^= w;
+  h *= 0xff51afd7ed558ccdULL;
+  return h ^ (h >> 33);
+}
+
+// Folds `n` bytes at `p`, with the call's tag and the byte count, into the
+// handle's set-up digest, eight bytes at a time.
+void digest(fdtd_ctx* c, int tag, const void* p, size_t n) {
+  unsigned long long h = mix64(c->setup_digest, ((unsigned long long)tag << 48) ^ (unsigned long long)n);
+  const unsigned char* b = (const unsigned char*)p;
+  size_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    unsigned long long w;
+    memcpy(&w, b + i, 8);
+    h = mix64(h, w);
+  }
+  unsigned long long t = 0;
+  for (; i < n; i++) t = (t << 8) | b[i];
+  c->setup_digest = mix64(h, t);
+}
+
+void digest_vals(fdtd_ctx* c, int tag, std::initializer_list<double> v) {
+  std::vector<double> a(v);
+  digest(c, tag, a.data(), a.size() * sizeof(double));
+}
+
 }  // namespace
 
 int fdtd_internal_traces(const fdtd_ctx* c, const double** V, const double** I, int* nsteps, int* steps,
@@ -670,6 +704,9 @@ int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
   c->nx = cfg->nx; c->ny = cfg->ny; c->nz = cfg->nz;
   c->dx = cfg->dx; c->dy = cfg->dy; c->dz = cfg->dz; c->dt = cfg->dt;
   c->nsteps = cfg->numberOfTimeSteps;
+  c->x_wall = c->prec == FDTD_PREC_F64 ? 0 : 1;
+  digest_vals(c, 1, {(double)c->nx, (double)c->ny, (double)c->nz, c->dx, c->dy, c->dz, c->dt, (double)c->nsteps,
+                     (double)c->prec});
   const long long nx = c->nx, ny = c->ny, nz = c->nz;
   c->ncomp[0] = (nx + 1) * ny * nz;
   c->ncomp[1] = nx * (ny + 1) * nz;
@@ -736,6 +773,8 @@ int fdtd_ctx_upload_coeff(fdtd_ctx* c, int which, const double* host, long n) {
   if (c->prec == FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "material-table problem takes fdtd_ctx_upload_material");
   if (which < 0 || which >= 18) return fail(FDTD_ERR_BADARG, "coefficient id %d out of range 0..17", which);
   if (n != coef_count(c, which)) return fail(FDTD_ERR_BADARG, "coefficient %d: got %ld values, expected %lld", which, n, coef_count(c, which));
+  digest_vals(c, 2, {(double)which});
+  digest(c, 2, host, (size_t)n * sizeof(double));
   CK(cudaSetDevice(c->device));
   int rc = upload_real(c, c->coef[which], host, n);
   if (!rc) c->coef_set[which] = true;
@@ -797,6 +836,12 @@ int fdtd_ctx_upload_cpml(fdtd_ctx* c, int f, int nc, const double* b_e, const do
   psi_sizes(c, f, nc, want);
   const double* cp[4] = {CPsi0, CPsi1, CPsi2, CPsi3};
   const long got[4] = {n0, n1, n2, n3};
+  digest_vals(c, 3, {(double)f, (double)nc, (double)m_start, (double)e_start, (double)n0, (double)n1, (double)n2,
+                     (double)n3});
+  for (const double* prof : {b_e, a_e, b_m, a_m, kappa_e, kappa_m})
+    if (prof && nc > 0) digest(c, 3, prof, (size_t)nc * sizeof(double));
+  for (int s = 0; s < 4; s++)
+    if (cp[s] && got[s] > 0) digest(c, 3, cp[s], (size_t)got[s] * sizeof(double));
   // FP64 coefficients built on the device and no CPsi given: CPsi and the
   // kappa division of the band are done here, on the device
   const bool dev = !table && c->coef_device && !CPsi0 && !CPsi1 && !CPsi2 && !CPsi3 && !n0 && !n1 && !n2 && !n3;
@@ -859,6 +904,10 @@ int fdtd_ctx_add_vsource(fdtd_ctx* c, int dir, const int* idx, const double* coe
   if (count <= 0) return fail(FDTD_ERR_BADARG, "source has no cells");
   if (nSteps < c->nsteps) return fail(FDTD_ERR_BADARG, "waveform has %d values, need %d", nSteps, c->nsteps);
   if ((int)c->src.size() >= kMaxSources) return fail(FDTD_ERR_BADARG, "at most %d sources", kMaxSources);
+  digest_vals(c, 4, {(double)dir, (double)count});
+  digest(c, 4, idx, (size_t)count * sizeof(int));
+  digest(c, 4, coef, (size_t)count * sizeof(double));
+  digest(c, 4, wave, (size_t)c->nsteps * sizeof(double));
   // component extents of E_dir
   const int ni = dir == 0 ? c->nx : c->nx + 1, nj = dir == 1 ? c->ny : c->ny + 1, nk = dir == 2 ? c->nz : c->nz + 1;
   const long long n = (long long)ni * nj * nk;
@@ -902,6 +951,8 @@ int fdtd_ctx_add_svoltage(fdtd_ctx* c, int dir, const int* idx, int count, doubl
   const long long n = c->ncomp[3 + dir];
   for (int q = 0; q < count; q++)
     if (idx[q] < 0 || idx[q] >= n) return fail(FDTD_ERR_BADARG, "probe index %d out of range", idx[q]);
+  digest_vals(c, 5, {(double)dir, (double)count, Csvf});
+  digest(c, 5, idx, (size_t)count * sizeof(int));
   CK(cudaSetDevice(c->device));
   HostVProbe p{dir, count, nullptr, Csvf};
   int rc = dalloc(c, (void**)&p.idx, count * sizeof(int));
@@ -920,6 +971,10 @@ int fdtd_ctx_add_scurrent(fdtd_ctx* c, const int* comp, const int* idx, const do
     if (comp[q] < 0 || comp[q] > 2) return fail(FDTD_ERR_BADARG, "current probe component %d not in 0..2", comp[q]);
     if (idx[q] < 0 || idx[q] >= c->ncomp[comp[q]]) return fail(FDTD_ERR_BADARG, "current probe index %d out of range", idx[q]);
   }
+  digest_vals(c, 6, {(double)count});
+  digest(c, 6, comp, (size_t)count * sizeof(int));
+  digest(c, 6, idx, (size_t)count * sizeof(int));
+  digest(c, 6, w, (size_t)count * sizeof(double));
   CK(cudaSetDevice(c->device));
   HostIProbe p{count, nullptr, nullptr, nullptr};
   int rc = dalloc(c, (void**)&p.comp, count * sizeof(int));
@@ -943,6 +998,8 @@ int fdtd_ctx_setup_farfield(fdtd_ctx* c, int nFreq, const double* freqs, int li,
   // the 4-point averages reach one cell outside the box on each side
   if (li < 2 || lj < 2 || lk < 2 || ui > c->nx || uj > c->ny || uk > c->nz || ui <= li || uj <= lj || uk <= lk)
     return fail(FDTD_ERR_BADARG, "Huygens box [%d,%d]x[%d,%d]x[%d,%d] does not fit the grid", li, ui, lj, uj, lk, uk);
+  digest_vals(c, 7, {(double)nFreq, (double)li, (double)lj, (double)lk, (double)ui, (double)uj, (double)uk});
+  digest(c, 7, freqs, (size_t)nFreq * sizeof(double));
   CK(cudaSetDevice(c->device));
   c->nFreq = nFreq;
   c->ffreq.assign(freqs, freqs + nFreq);
@@ -987,6 +1044,9 @@ int fdtd_ctx_upload_material(fdtd_ctx* c, int comp, const unsigned char* ids, lo
   if (rows < 1 || rows > kTableRows) return fail(FDTD_ERR_BADARG, "table rows %d not in 1..%d", rows, kTableRows);
   for (long q = 0; q < n; q++)
     if (ids[q] >= rows) return fail(FDTD_ERR_BADARG, "material id %d >= table rows %d", ids[q], rows);
+  digest_vals(c, 8, {(double)comp, (double)rows});
+  digest(c, 8, ids, (size_t)n);
+  digest(c, 8, table, (size_t)rows * 3 * sizeof(double));
   CK(cudaSetDevice(c->device));
   CK(xfer(c, c->ids[comp], ids, n, cudaMemcpyHostToDevice));
   int rc = set_rows(c, comp, std::vector<double>(table, table + 3 * rows));
@@ -1037,6 +1097,13 @@ int fdtd_ctx_build_material(fdtd_ctx* c, const unsigned char* mat, long ncells, 
   unsigned char mmax = 0;
   for (long q = 0; q < ncells; q++) mmax = std::max(mmax, mat[q]);
   if (mmax >= ntypes) return fail(FDTD_ERR_BADARG, "material id %d has no properties", mmax);
+  digest_vals(c, 9, {(double)ncells, (double)ntypes, (double)nplates});
+  digest(c, 9, mat, (size_t)ncells);
+  digest(c, 9, props, (size_t)ntypes * 4 * sizeof(double));
+  if (nplates > 0) {
+    digest(c, 9, plates, (size_t)nplates * 7 * sizeof(int));
+    digest(c, 9, plate_sigma, (size_t)nplates * sizeof(double));
+  }
   MatBuild b{};
   b.nx = c->nx; b.ny = c->ny; b.nz = c->nz; b.M = ntypes; b.nplates = nplates;
   std::vector<double> psig;  // distinct plate conductivities
@@ -1199,6 +1266,11 @@ static int override_coef64(fdtd_ctx* c, int comp, const int* idx, const double* 
 
 int fdtd_ctx_override_material(fdtd_ctx* c, int comp, const int* idx, const double* triples, int count) {
   if (!c || !idx || !triples) return fail(FDTD_ERR_BADARG, "NULL argument");
+  if (count > 0) {
+    digest_vals(c, 10, {(double)comp, (double)count});
+    digest(c, 10, idx, (size_t)count * sizeof(int));
+    digest(c, 10, triples, (size_t)count * 3 * sizeof(double));
+  }
   if (c->prec == FDTD_PREC_F64) return override_coef64(c, comp, idx, triples, count);
   if (c->prec != FDTD_PREC_F32_TABLE) return fail(FDTD_ERR_STATE, "not a material-table or FP64 problem");
   if (comp < 0 || comp > 5 || !c->ids_set[comp]) return fail(FDTD_ERR_STATE, "component %d has no material ids yet", comp);
@@ -1369,10 +1441,11 @@ int fdtd_ctx_read_farfield(fdtd_ctx* c, int array, double* re, double* im, long 
 namespace {
 
 struct StateHeader {
-  char magic[8];  // "FDTDST1\0"
+  char magic[8];  // "FDTDST2\0"
   int nx, ny, nz, prec, nsteps, ts, nv, ni, nfreq, kahan;
   long long psi[6][4];
   long long ff_values;
+  unsigned long long setup;  // the handle's set-up digest
   long long bytes;  // whole state, header included
 };
 
@@ -1394,12 +1467,13 @@ std::vector<std::pair<void*, size_t>> state_ranges(fdtd_ctx* c) {
 
 StateHeader state_header(fdtd_ctx* c) {
   StateHeader h{};
-  memcpy(h.magic, "FDTDST1", 8);
+  memcpy(h.magic, "FDTDST2", 8);
   h.nx = c->nx; h.ny = c->ny; h.nz = c->nz; h.prec = c->prec; h.nsteps = c->nsteps; h.ts = c->ts;
   h.nv = (int)c->vprobe.size(); h.ni = (int)c->iprobe.size(); h.nfreq = c->nFreq; h.kahan = c->acc_kahan;
   for (int f = 0; f < 6; f++)
     for (int s = 0; s < 4; s++) h.psi[f][s] = (c->face[f].present && c->face[f].psi[s]) ? c->face[f].n[s] : 0;
   h.ff_values = c->nFreq > 0 ? c->ffoff[23] + 2LL * c->nFreq * c->ffsz[2] : 0;
+  h.setup = c->setup_digest;
   long long bytes = sizeof(StateHeader);
   for (auto& q : state_ranges(c)) bytes += (long long)q.second;
   h.bytes = bytes;
@@ -1442,8 +1516,11 @@ int fdtd_ctx_load_state(fdtd_ctx* c, const void* buf, long long bytes) {
   StateHeader mine = state_header(c), theirs;
   if (bytes < (long long)sizeof(StateHeader)) return fail(FDTD_ERR_BADARG, "state buffer too small");
   memcpy(&theirs, buf, sizeof(theirs));
-  if (memcmp(theirs.magic, "FDTDST1", 8) != 0) return fail(FDTD_ERR_BADARG, "not an engine state");
+  if (memcmp(theirs.magic, "FDTDST2", 8) != 0) return fail(FDTD_ERR_BADARG, "not an engine state");
   mine.ts = theirs.ts;  // the step is what loading changes
+  if (theirs.setup != mine.setup)
+    return fail(FDTD_ERR_BADARG, "state was saved from a handle set up with other data (grid, dt, coefficients, "
+                                 "faces, sources, probes or far field)");
   if (memcmp(&mine, &theirs, sizeof(StateHeader)) != 0 || bytes != theirs.bytes)
     return fail(FDTD_ERR_BADARG, "state was saved from a problem of another shape, precision or probe set");
   if (theirs.ts < 0 || theirs.ts > c->nsteps) return fail(FDTD_ERR_BADARG, "state step %d out of range", theirs.ts);
@@ -1489,6 +1566,20 @@ int fdtd_ctx_set_dft_accumulator(fdtd_ctx* c, int kahan_fp32) {
   if (c->ts != 0) return fail(FDTD_ERR_STATE, "the accumulator mode is set before the first step");
   c->acc_kahan = kahan_fp32;
   invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_set_x_wall(fdtd_ctx* c, int wall) {
+  if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
+  if (wall != 0 && wall != 1) return fail(FDTD_ERR_BADARG, "x wall mode %d not in {0,1}", wall);
+  c->x_wall = wall;
+  invalidate(c);
+  return FDTD_OK;
+}
+
+int fdtd_ctx_get_x_wall(const fdtd_ctx* c, int* wall) {
+  if (!c || !wall) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *wall = c->x_wall;
   return FDTD_OK;
 }
 

@@ -159,6 +159,11 @@ struct StepParams {
   int bands_disjoint;  // per axis, no position lies in both CPML bands (H and E)
   int dft_block;       // time-blocked surface DFT: steps per block (0: per step)
   int* dft_done;       // steps the blocked DFT has accumulated
+  // 0: Ey and Ez at i = nx are bulk-updated from the values the reference
+  // reads one plane past Hz and Hy (fdtd_kernels.ts:159-204); 1: they are not
+  // updated and stay zero, the ranges of the MATLAB original
+  // (fdtd_solve_Ch9_ex9a_12032026.m.txt:2095-2106), a PEC wall.
+  int x_wall;
 };
 
 // Band of a face that contains `pos` (H: m band, E: e band): ci or -1.
@@ -888,6 +893,7 @@ __device__ __forceinline__ void e_plane(const StepParams<T, C>& p, const ECol<T>
   const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
   const Fields<T>& f = p.f;
   const bool inx = i < nx;
+  const bool wall = !inx && p.x_wall;  // Ey, Ez at i = nx held at zero
   // Hz(i,j,k) and Hy(i,j,k); at i = nx the reference reads Ex(0,j,k) after its
   // bulk update and the start of the Hz array instead (one plane past Hz / Hy)
   T hz_i = T(0), hy_i = T(0);
@@ -918,7 +924,7 @@ __device__ __forceinline__ void e_plane(const StepParams<T, C>& p, const ECol<T>
     f.Ex[idx] = e;
   }
   // Ey (nx+1, ny, nz+1): bulk on i in [1,nx], k in [1,nz)
-  if (c.ey_ok) {
+  if (c.ey_ok && !wall) {
     const int idx = i * sHzEy + c.ob;
     T e = f.Ey[idx];
     T dhx = T(0), dhz = T(0);
@@ -937,7 +943,7 @@ __device__ __forceinline__ void e_plane(const StepParams<T, C>& p, const ECol<T>
     f.Ey[idx] = e;
   }
   // Ez (nx+1, ny+1, nz): bulk on i in [1,nx], j in [1,ny)
-  if (c.ez_ok) {
+  if (c.ez_ok && !wall) {
     const int idx = i * sHyEz + c.oa;
     T e = f.Ez[idx];
     T dhy = T(0), dhx = T(0);
@@ -1196,7 +1202,8 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     if (c.sx) inject_masked(p.src, c.sx, i, c.j, c.k, ts, e);
     f.Ex[i * sEx + c.ob] = e;
   }
-  if (c.ey_ok) {
+  const bool wall = i >= nx && p.x_wall;  // Ey, Ez at i = nx held at zero
+  if (c.ey_ok && !wall) {
     T e = in.ey;
     const T dhx = c.kz ? A::dif(in.hx_c, in.hx_km) : T(0);
     const T dhz = i >= 1 ? A::dif(in.hz_i, hz_p) : T(0);
@@ -1213,7 +1220,7 @@ __device__ __forceinline__ void e_band_store(const StepParams<T, C>& p, const EC
     if (c.sy) inject_masked(p.src, c.sy, i, c.j, c.k, ts, e);
     f.Ey[i * sHzEy + c.ob] = e;
   }
-  if (c.ez_ok) {
+  if (c.ez_ok && !wall) {
     T e = in.ez;
     const T dhy = i >= 1 ? A::dif(in.hy_i, hy_p) : T(0);
     const T dhx = c.jy ? A::dif(in.hx_c, in.hx_jm) : T(0);

@@ -327,6 +327,22 @@ def test_state_checkpoint_resumes_bit_identically(precision):
     with Engine(other, precision) as c:
         with pytest.raises(N.FdtdError):
             c.load_state(state)
+    # same shape and probe set, other physics: a different dt, then another
+    # permittivity in one material
+    import copy
+    for change in ("dt", "eps"):
+        scn2 = copy.deepcopy(scn)
+        if change == "dt":
+            scn2["courantFactor"] = 0.8
+        else:
+            scn2["materialTypes"][3]["eps_r"] += 0.5       # the block that fills the box
+        p2 = build_problem_from_scenario(scn2, steps, per_cell=(precision == "f64"))
+        assert (p2.grid.nx, p2.grid.ny, p2.grid.nz) == (p.grid.nx, p.grid.ny, p.grid.nz)
+        with Engine(p2, precision) as c:
+            with pytest.raises(N.FdtdError) as ei:
+                c.load_state(state)
+            assert ei.value.code == N.FDTD_ERR_BADARG
+            assert "other data" in str(ei.value), change
 
 
 @pytest.mark.parametrize("acc", ["f64", "kahan-f32"])
