@@ -144,39 +144,59 @@ def ncu_traffic(workload: str):
     return None
 
 
-def cpu_oracle_rate(n=(256, 256, 256), budget_s: float = 15.0) -> dict:
+def _host_ram_ok(n, factor: float = 1.5) -> bool:
+    """Whether the host can hold the oracle's FP64 fields and 18 per-cell
+    coefficient arrays of an n-cell box (with `factor` headroom)."""
+    need = 8 * 26 * int(np.prod(n))
+    try:
+        avail = next(int(l.split()[1]) * 1024 for l in open("/proc/meminfo") if l.startswith("MemAvailable"))
+    except (OSError, StopIteration, ValueError):
+        return False
+    return avail > factor * need
+
+
+def cpu_oracle_rate(n=(256, 256, 256), budget_s: float = 15.0, steps: int | None = None, warm: int = 5,
+                    max_steps: int = 390, one_thread: bool = True) -> dict:
     """The CPU oracle (C restatement of the reference's FP64 loop, OpenMP over
-    all host cores) on a bounded sample of the scaling-box workload."""
+    all host cores) on a bounded sample of the scaling-box workload: `steps`
+    steps, or as many as fit `budget_s` (at most max_steps), after `warm`."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     _package()
     from special_topics_b200 import workloads
-    scn = workloads.scaling_box(n, seed=1, steps=400)
+    total = warm + (steps or max_steps) + 3
+    scn = workloads.scaling_box(n, seed=1, steps=total)
     threads = os.cpu_count() or 1
-    o = oracle.Oracle(scn, 400, threads=threads)
-    o.step(2)
+    t = time.perf_counter()
+    o = oracle.Oracle(scn, total, threads=threads)
+    setup_s = time.perf_counter() - t
+    o.step(max(0, warm - 3))
     t = time.perf_counter()
     o.step(3)
     per = (time.perf_counter() - t) / 3
-    k = int(max(3, min(390, budget_s / max(per, 1e-6))))
+    k = steps or int(max(1, min(max_steps, budget_s / max(per, 1e-6))))
     t = time.perf_counter()
     o.step(k)
     dt = time.perf_counter() - t
     cells = o.nx * o.ny * o.nz
     del o
-    # the same sample on one thread, a few steps
-    o1 = oracle.Oracle(scn, 400, threads=1)
-    o1.step(1)
-    t = time.perf_counter()
-    o1.step(2)
-    one = cells * 2 / (time.perf_counter() - t) / 1e9
+    one = None
+    if one_thread:
+        # the same sample on one thread, a few steps
+        o1 = oracle.Oracle(scn, total, threads=1)
+        o1.step(1)
+        t = time.perf_counter()
+        o1.step(2)
+        one = cells * 2 / (time.perf_counter() - t) / 1e9
+        del o1
     cpu = ""
     try:
         cpu = next(l.split(":", 1)[1].strip() for l in open("/proc/cpuinfo") if l.startswith("model name"))
     except (OSError, StopIteration):
         pass
     return {"value": cells * k / dt / 1e9, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"scaling box {n[0]}x{n[1]}x{n[2]} ({cells} cells), {k} FP64 steps timed after 5 warm-up steps",
+            "sample": f"scaling box {n[0]}x{n[1]}x{n[2]} ({cells} cells), {k} FP64 steps timed after {warm} warm-up steps",
+            "ms_per_step": dt / k * 1e3, "setup_s": setup_s,
             "one_thread_value": one, "cpu_model": cpu}
 
 
@@ -203,21 +223,38 @@ def main():
                     help="fixed batch shape chunk,rows,prefetch,group[,streams[,width]] (skips the tuner)")
     ap.add_argument("--ttS11-members", dest="ttS11_members", type=int, default=64,
                     help="held-out variants of the time-to-S11 leg (0: skip)")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 128^3..512x512x640 FP32/FP64 sweep")
+    ap.add_argument("--no-config0", action="store_true", help="skip the 0.5 mm inverted-F antenna leg")
+    ap.add_argument("--cpu-sweep", action="store_true",
+                    help="only time the CPU oracle for 50 steps at each sweep size (long; needs about 40 GB RAM)")
     args = ap.parse_args()
     n = tuple(int(x) for x in args.grid.split("x"))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     workload = f"scaling-box-{args.grid}"
+    config = {"workload": workload, "grid": list(n), "cells": int(np.prod(n)), "ncpml": args.ncpml,
+              "far_field_freqs": 2,
+              "l2": "inputs larger than L2 (fields and ids >> 126 MB), no flush needed",
+              "parallelism": f"{args.gpus} independent problem(s), one per GPU"}
+
+    if args.cpu_sweep:
+        if rank == 0:
+            print(json.dumps({"cpu_sweep": [cpu_oracle_rate(g, steps=50, warm=2) for g in SWEEP_GRIDS]}), flush=True)
+        return
 
     if args.impl == "reference":
         if rank != 0:
             return
-        base = cpu_oracle_rate()
+        # the reference's FP64 CPU loop (the oracle) on this same grid when the
+        # host holds its per-cell arrays, else on a 256^3 sample of the workload
+        grid = n if _host_ram_ok(n) else (256, 256, 256)
+        base = cpu_oracle_rate(grid, budget_s=20.0, max_steps=max(1, args.steps))
         line = {"metric": METRIC, "value": base["value"], "unit": "Gcell-updates/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload, "precision": "f64 (reference CPU path)"},
+                "config": dict(config) if grid == n else dict(config, workload=f"scaling-box-{grid[0]}x{grid[1]}x{grid[2]}",
+                                                                grid=list(grid), cells=int(np.prod(grid))),
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -330,11 +367,11 @@ def main():
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision != "f64" else "f64",
         "data": "synthetic (seeded scaling-box scenario in the reference's JSON schema)",
-        "config": {"workload": workload, "cells": cells, "precision": args.precision,
-                   "time_steps_in_problem": K + W + P, "far_field_freqs": 2,
-                   "far_field_dft": f"time-blocked, {dft_block} steps per block" if dft_block else "every step",
-                   "l2": "inputs larger than L2 (fields and ids >> 126 MB), no flush needed",
-                   "parallelism": f"{world} independent problem(s), one per GPU"},
+        "config": config,
+        "setup": {"precision": args.precision, "time_steps_in_problem": K + W + P,
+                  "far_field_dft": f"time-blocked, {dft_block} steps per block" if dft_block else "every step",
+                  "x_wall": "Ey, Ez at i = nx held at zero (FP32 default)" if args.precision != "f64"
+                            else "the reference's reads at i = nx"},
         "roofline": {"bound": "hbm", "kernel": f"k_step_{dom}", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "frac_of_nominal_8TBs": achieved / NOMINAL_HBM_GBS,
@@ -367,12 +404,26 @@ def main():
                           scaling="strong: the members are split over the ranks")
         if rank == 0 and bs:
             line["batched"] = bs
+    if rank == 0 and world == 1 and not args.no_config0:
+        try:
+            line["config0"] = config0_side(device=local)
+        except Exception as e:  # a side leg must not hide the main number
+            line["config0"] = {"error": str(e)}
+    if rank == 0 and world == 1 and not args.no_sweep:
+        try:
+            t64 = None
+            if not args.no_fp64:
+                line["fp64_plain"] = fp64_side(pkg)
+                t64 = line["fp64_plain"]["tiling"]
+            line["scaling_sweep"] = scaling_sweep_side(tuning, t64, device=local, dft_block=dft_block)
+        except Exception as e:
+            line["scaling_sweep"] = {"error": str(e)}
     if rank == 0 and world == 1 and args.ttS11_members > 0:
         try:
             line["time_to_s11"] = time_to_s11_side(args.ttS11_members, device=local, dft_block=args.dft_block)
         except Exception as e:  # this leg must not hide the main number
             line["time_to_s11"] = {"error": str(e)}
-    if rank == 0 and world == 1 and not args.no_fp64:
+    if rank == 0 and world == 1 and not args.no_fp64 and "fp64_plain" not in line:
         line["fp64_plain"] = fp64_side(pkg)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -558,6 +609,109 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     net.close()
     out["ratio_plain_f64_over_learned"] = out["plain_f64_s"] / out["learned"]["time_s"]
     out["ratio_plain_f64_over_no_network"] = out["plain_f64_s"] / out["no_network"]["time_s"]
+    return out
+
+
+SWEEP_GRIDS = ((128, 128, 128), (256, 256, 256), (384, 384, 384), (512, 512, 640))
+L2_BYTES = 126 * 2**20
+
+
+def _leg(p, precision: str, K: int, W: int, tiling: dict | None, device: int = 0, dft_block: int = 0) -> dict:
+    """One device-timed run: K steps after W warm-up steps, Gcell/s and the
+    dominant step kernel against the HBM roofline."""
+    from special_topics_b200 import autotune
+    from special_topics_b200.backend import Engine
+    with Engine(p, precision, device=device, dft_block=dft_block) as eng:
+        if tiling:
+            autotune.set_tiling(eng, tiling["chunk"], tiling["rows"], tiling.get("prefetch", 1), tiling.get("width", 32))
+        eng.run(W)
+        ms = eng.run_timed(K)
+        kern = eng.profile_kernels(8)
+    byts = algorithmic_bytes(p, precision)
+    peak, peak_kind = hbm_peak()
+    dom = "e" if kern["e"] >= kern["h"] else "h"
+    ach = byts[dom] / (kern[dom] / 1e3) / 1e9
+    return {"precision": precision, "value": p.grid.cells * K / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s",
+            "steps": K, "ms_per_step": ms / K, "kernel_ms": kern,
+            "roofline": {"kernel": f"k_step_{dom}", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+                         "frac": ach / peak, "algorithmic_bytes_per_launch": byts[dom]}}
+
+
+def scaling_sweep_side(tiling32: dict | None, tiling64: dict | None, device: int = 0, dft_block: int = 0,
+                       grids=SWEEP_GRIDS) -> list:
+    """configs[1] at every size in FP32 material tables and FP64 (per-cell
+    coefficients built on the device, bit-identical to the host-built ones).
+    About 2 G cell-updates are timed per leg (at least 20 steps).  Grids whose
+    FP32 working set fits the 126 MB L2 are marked L2-resident: their rate is
+    not an HBM figure."""
+    from special_topics_b200 import workloads
+    from special_topics_b200.scenario import build_problem_from_scenario
+    out = []
+    for n in grids:
+        cells = n[0] * n[1] * n[2]
+        K = int(min(1000, max(20, 2e9 // cells)))
+        W = 68                      # the 64-step graph is captured and warmed before the timed steps
+        p = build_problem_from_scenario(workloads.scaling_box(n, seed=1, steps=K + W + 8), K + W + 8, per_cell=False)
+        for prec, tiling in (("f32-table", tiling32), ("f64", tiling64)):
+            leg = _leg(p, prec, K, W, tiling, device, dft_block if prec != "f64" else 0)
+            work = algorithmic_bytes(p, prec)
+            leg.update({"grid": list(n), "cells": cells,
+                        "l2_resident": bool(work["e"] < L2_BYTES),
+                        "tiling": {k: tiling.get(k) for k in ("chunk", "rows", "prefetch", "width")} if tiling else "default"})
+            out.append(leg)
+        del p
+    return out
+
+
+def config0_side(device: int = 0, oracle_steps: int = 1000) -> dict:
+    """The north_star's parity scenario: the 0.5 mm inverted-F antenna (39 x 136
+    x 136, 7000 steps, far field at 2.4 GHz).  Device-timed FP64 (the drop-in)
+    and FP32-table runs of the whole 7000 steps; time-to-S11 (301 points,
+    1-4 GHz) from the first step launch to S11 on the host for each; the CPU
+    oracle on the box's cores for `oracle_steps` steps of the same scenario
+    (extrapolated to 7000, stated), whose traces must equal the FP64 run's
+    first steps bit for bit."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from special_topics_b200 import earlystop as ES
+    from special_topics_b200 import workloads
+    from special_topics_b200.backend import Engine
+    from special_topics_b200.scenario import build_problem_from_scenario
+    steps = 7000
+    scn = workloads.ifa_config0(steps)
+    p64 = build_problem_from_scenario(scn, steps)
+    p32 = build_problem_from_scenario(scn, steps, per_cell=False)
+    cells = p64.grid.cells
+    out = {"workload": scn["name"], "grid": [p64.grid.nx, p64.grid.ny, p64.grid.nz], "cells": cells, "steps": steps,
+           "l2_resident": True}
+    s11 = {}
+    for name, prob, prec in (("f64", p64, "f64"), ("f32_table", p32, "f32-table")):
+        with Engine(prob, prec, device=device) as eng:
+            start = eng.save_state()        # step 0
+            eng.run(64)                     # captures and warms the step graph
+            eng.load_state(start)           # back to step 0: the timed run is the whole run
+            t0 = time.perf_counter()
+            ms = eng.run_timed(steps)
+            V, I = eng.voltages()[0], eng.currents()[0]
+            s11[name] = ES.s11_db(V, I, prob.grid.dt, ES.S11_FREQS)
+            tt = time.perf_counter() - t0
+            if name == "f64":
+                v64 = V
+        out[name] = {"value": cells * steps / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "device_ms": ms,
+                     "time_to_s11_s": tt}
+    out["f32_table"]["s11_max_abs_dB_vs_f64"] = float(np.abs(s11["f32_table"] - s11["f64"]).max())
+    out["time_to_s11_ratio_f64_over_f32_table"] = out["f64"]["time_to_s11_s"] / out["f32_table"]["time_to_s11_s"]
+    threads = os.cpu_count() or 1
+    o = oracle.Oracle(scn, steps, threads=threads)
+    t0 = time.perf_counter()
+    o.step(oracle_steps)
+    dt = time.perf_counter() - t0
+    same = bool(np.array_equal(o.get("V:0")[:oracle_steps], v64[:oracle_steps]))
+    del o
+    out["cpu_oracle"] = {"value": cells * oracle_steps / dt / 1e9, "unit": "Gcell-updates/s", "cores": threads,
+                         "kind": "port", "steps_timed": oracle_steps, "s_per_7000_steps_extrapolated": dt * steps / oracle_steps,
+                         "v_trace_bit_identical_to_gpu_f64": same}
+    out["time_to_s11_ratio_cpu_oracle_over_f64"] = out["cpu_oracle"]["s_per_7000_steps_extrapolated"] / out["f64"]["time_to_s11_s"]
     return out
 
 
