@@ -220,7 +220,7 @@ def main():
     ap.add_argument("--batch-members", type=int, default=128, help="inverted-F variants in the batched sweep (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the batched sweep")
     ap.add_argument("--batch-tiling", default=None,
-                    help="fixed batch shape chunk,rows,prefetch,group[,streams[,width]] (skips the tuner)")
+                    help="fixed batch shape chunk,rows,prefetch,group[,streams[,width[,per_launch]]] (skips the tuner)")
     ap.add_argument("--ttS11-members", dest="ttS11_members", type=int, default=64,
                     help="held-out variants of the time-to-S11 leg (0: skip)")
     ap.add_argument("--no-sweep", action="store_true", help="skip the 128^3..512x512x640 FP32/FP64 sweep")
@@ -477,13 +477,14 @@ def _sum_over_ranks(x: float, dist, local: int) -> float:
 def _best_by_mode(table: list) -> dict:
     """Fastest tuned step time (ms) of the tile-list and member-kernel modes."""
     out = {}
-    for name, pick in (("tile_list", lambda r: r.get("streams", 0) == 0),
+    for name, pick in (("tile_list", lambda r: r.get("streams", 0) == 0 and r.get("per_launch", 0) == 0),
+                       ("grouped", lambda r: r.get("streams", 0) == 0 and r.get("per_launch", 0) > 0),
                        ("member_kernels", lambda r: r.get("streams", 0) > 0)):
         rows = [r for r in table if pick(r)]
         if rows:
             b = min(rows, key=lambda r: r["ms_per_step"])
-            out[name] = {k: b[k] for k in ("ms_per_step", "chunk", "rows", "prefetch", "group", "streams", "width")
-                         if k in b}
+            out[name] = {k: b[k] for k in ("ms_per_step", "chunk", "rows", "prefetch", "group", "streams", "width",
+                                           "per_launch") if k in b}
     return out
 
 
@@ -503,7 +504,8 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
         with Batch(engs) as b:
             if fixed:
                 v = [int(x) for x in fixed.split(",")]
-                b.set_tiling(v[0], v[1], v[2], v[3], v[4] if len(v) > 4 else 0, v[5] if len(v) > 5 else 32)
+                b.set_tiling(v[0], v[1], v[2], v[3], v[4] if len(v) > 4 else 0, v[5] if len(v) > 5 else 32,
+                             v[6] if len(v) > 6 else 0)
                 tuning = {"ms_per_step": None}
             else:
                 tuning = autotune.tune_batch(b, steps_per_candidate=tune_steps)
@@ -532,6 +534,11 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
         # (mid-step and epilogue time included, so conservative)
         roof_kernel = f"k_step_h + k_step_e of every member on {tiling['streams']} streams (whole step)"
         roof_bytes, roof_ms = byts["h"] + byts["e"], ms / K
+    elif tiling.get("per_launch", 0) > 0:
+        ngroups = -(-len(problems) // tiling["per_launch"])
+        roof_kernel = (f"k_batch_group ({dom.upper()}): {ngroups} launches of {tiling['per_launch']} members "
+                       "side by side, timed together")
+        roof_bytes, roof_ms = byts[dom], kern[dom]
     else:
         roof_kernel = f"k_batch_half ({dom.upper()})"
         roof_bytes, roof_ms = byts[dom], kern[dom]
@@ -543,7 +550,9 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
             "grid_max": list(max(dims, key=lambda d: d[0] * d[1] * d[2])),
             "value": cells * K / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "steps": K, "warmup": W,
             "ms_per_step": ms / K,
-            "gpu_launches": (5 if dft_block else 4) * K * (len(problems) if tiling.get("streams", 0) else 1),
+            "gpu_launches": K * ((5 if dft_block else 4) * len(problems) if tiling.get("streams", 0) else
+                                 (3 if dft_block else 2) + 2 * (-(-len(problems) // tiling["per_launch"])
+                                                                if tiling.get("per_launch", 0) else 1)),
             "kernel_ms": kern,
             "tiling": tiling, "tuning_ms_per_step": tuning["ms_per_step"],
             "tuning_best_ms_by_mode": _best_by_mode(tuning.get("table", [])),

@@ -244,6 +244,14 @@ int fdtd_batch_set_streams(fdtd_batch* batch, int streams);
 int fdtd_batch_set_block_width(fdtd_batch* batch, int threads_along_k);
 int fdtd_batch_get_block_width(const fdtd_batch* batch, int* threads_along_k);
 int fdtd_batch_get_streams(const fdtd_batch* batch, int* streams);
+/* Grouped mode (used when streams is 0): members > 0 carries that many
+ * members' parameter blocks (at most 22) as the parameter of one launch, in
+ * member order, so the step kernels read them from the constant bank as a
+ * single problem's launch does; the group launches of a half-step run side by
+ * side on worker streams.  0 (default) = the tile-list or persistent launches
+ * of fdtd_batch_set_tiling.  Results do not depend on the mode. */
+int fdtd_batch_set_members_per_launch(fdtd_batch* batch, int members);
+int fdtd_batch_get_members_per_launch(const fdtd_batch* batch, int* members);
 /* Runs `count` steps of every member.  All members must be at the same step and
  * have `count` steps left.  Returns FDTD_ERR_NONFINITE naming the first member
  * whose watchdog fired. */

@@ -43,6 +43,7 @@ EXPORTS = (
     "fdtd_ctx_set_dft_block", "fdtd_batch_set_streams", "fdtd_batch_get_streams",
     "fdtd_ctx_set_block_width", "fdtd_ctx_get_block_width", "fdtd_batch_set_block_width",
     "fdtd_batch_get_block_width", "fdtd_ctx_set_x_wall", "fdtd_ctx_get_x_wall",
+    "fdtd_batch_set_members_per_launch", "fdtd_batch_get_members_per_launch",
 )
 
 
@@ -135,6 +136,8 @@ def lib() -> C.CDLL:
     L.fdtd_ctx_set_dft_accumulator.argtypes = [v, i]
     L.fdtd_ctx_set_dft_block.argtypes = [v, i]
     L.fdtd_ctx_set_x_wall.argtypes = [v, i]
+    L.fdtd_batch_set_members_per_launch.argtypes = [v, i]
+    L.fdtd_batch_get_members_per_launch.argtypes = [v, ip]
     L.fdtd_ctx_get_x_wall.argtypes = [v, ip]
     L.fdtd_ctx_state_size.argtypes = [v, P(C.c_longlong)]
     L.fdtd_ctx_save_state.argtypes = [v, v, C.c_longlong]

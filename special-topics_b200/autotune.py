@@ -102,6 +102,9 @@ BATCH_GROUPS = (0, 1, 2, 4, 8, 16)
 BATCH_STREAMS = (2, 3, 4, 6, 8, 16)
 MEMBER_SHAPES = ((32, 4, 1), (16, 4, 1), (32, 8, 1), (64, 4, 1))
 MEMBER_STEPS = 64   # member-kernel trials time whole graphs of this many steps
+# grouped mode: members per launch, then launch shapes (rows, width, prefetch) at the best count
+PER_LAUNCH = (8, 11, 16, 22)
+GROUPED_SHAPES = ((4, 32), (8, 32), (16, 32), (8, 16), (16, 16))
 
 
 def batch_key(batch) -> str:
@@ -117,7 +120,8 @@ def batch_steps_needed(steps_per_candidate: int, precision: str = "f32-table") -
     tile_mode = 2 * steps_per_candidate * (len(BATCH_CHUNKS) * len(ROWS) * len(prefetch_depths(precision))
                                            + len(BATCH_GROUPS))
     member_mode = 2 * MEMBER_STEPS * (len(BATCH_STREAMS) + len(MEMBER_SHAPES))
-    return tile_mode + 2 * steps_per_candidate * len(NARROW_ROWS) + member_mode
+    grouped = 2 * steps_per_candidate * (len(PER_LAUNCH) + len(GROUPED_SHAPES) * len(prefetch_depths(precision)))
+    return tile_mode + 2 * steps_per_candidate * len(NARROW_ROWS) + member_mode + grouped
 
 
 def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> dict:
@@ -125,7 +129,9 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
     the same values, so tuning only advances the members by
     batch_steps_needed(steps_per_candidate) steps).  Tile-list mode: x planes
     per thread, block rows and prefetch depth with one block per tile, then
-    the tile group of the persistent grid.  Member-kernel mode: the worker
+    the tile group of the persistent grid.  Grouped mode: the members per
+    launch at the best tile-list shape, then block shapes and prefetch depths
+    at the best count.  Member-kernel mode: the worker
     stream count at the first member shape, then the member shapes at the best
     count (whole graphs of MEMBER_STEPS steps, since a member-mode step is
     many launches).  Sets and returns the fastest."""
@@ -133,17 +139,18 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
     cache = _load()
     if use_cache and key in cache:
         r = cache[key]
-        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"], r.get("streams", 0), r.get("width", 32))
+        batch.set_tiling(r["chunk"], r["rows"], r["prefetch"], r["group"], r.get("streams", 0), r.get("width", 32),
+                         r.get("per_launch", 0))
         return r
     max_x = max(e.problem.grid.nx for e in batch.engines) + 1
     table = []
 
-    def trial(chunk, rows, pf, group, streams=0, steps=steps_per_candidate, width=32):
-        batch.set_tiling(chunk, rows, pf, group, streams, width)
+    def trial(chunk, rows, pf, group, streams=0, steps=steps_per_candidate, width=32, per_launch=0):
+        batch.set_tiling(chunk, rows, pf, group, streams, width, per_launch)
         batch.run_timed(steps)              # capture and warm the graph
         ms = batch.run_timed(steps) / steps
         table.append({"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams,
-                      "width": width, "ms_per_step": ms})
+                      "width": width, "per_launch": per_launch, "ms_per_step": ms})
 
     for chunk in BATCH_CHUNKS:
         for rows in ROWS:
@@ -155,6 +162,13 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
     best = min(table, key=lambda r: r["ms_per_step"])
     for group in BATCH_GROUPS[1:]:
         trial(best["chunk"], best["rows"], best["prefetch"], group, width=best["width"])
+    tl = min(table, key=lambda r: r["ms_per_step"])
+    for per in PER_LAUNCH:
+        trial(tl["chunk"], tl["rows"], tl["prefetch"], 0, width=tl["width"], per_launch=per)
+    p_best = min((r for r in table if r["per_launch"] > 0), key=lambda r: r["ms_per_step"])["per_launch"]
+    for rw, wd in GROUPED_SHAPES:
+        for pf in prefetch_depths(batch.engines[0].precision):
+            trial(max_x, rw, pf, 0, width=wd, per_launch=p_best)
     ch, rw, pf = MEMBER_SHAPES[0]
     for streams in BATCH_STREAMS:
         trial(min(ch, max_x), rw, pf, 0, streams, MEMBER_STEPS)
@@ -163,7 +177,8 @@ def tune_batch(batch, steps_per_candidate: int = 16, use_cache: bool = True) -> 
         trial(min(ch, max_x), rw, pf, 0, s_best, MEMBER_STEPS)
     best = min(table, key=lambda r: r["ms_per_step"])
     out = dict(best, table=table)
-    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"], best["streams"], best["width"])
+    batch.set_tiling(best["chunk"], best["rows"], best["prefetch"], best["group"], best["streams"], best["width"],
+                     best["per_launch"])
     cache[key] = out
     os.makedirs(os.path.dirname(CACHE), exist_ok=True)
     with open(CACHE, "w") as f:

@@ -263,9 +263,11 @@ class Engine:
 class Batch:
     """Engines of one precision on one device advanced together
     (fdtd_batch_* in include/fdtd_b200.h).  streams = 0: every step is four
-    launches for the whole batch over a tile list; streams = S > 0: each
-    member's own step kernels on S worker streams in one graph.  The engines
-    stay usable for readback and must outlive the batch."""
+    launches for the whole batch over a tile list, or, with per_launch = P > 0,
+    H and E launches that each carry P members' parameter blocks as their
+    kernel parameter (grouped mode); streams = S > 0: each member's own step
+    kernels on S worker streams in one graph.  The engines stay usable for
+    readback and must outlive the batch."""
 
     def __init__(self, engines: list, chunk: int = 8, rows: int = 4, prefetch: int = 1, group: int = 0,
                  streams: int = 0):
@@ -279,28 +281,33 @@ class Batch:
         self.set_tiling(chunk, rows, prefetch, group, streams)
 
     def set_tiling(self, chunk: int, rows: int, prefetch: int = 1, group: int = 0, streams: int | None = None,
-                   width: int | None = None) -> None:
+                   width: int | None = None, per_launch: int | None = None) -> None:
         """Launch shape (see fdtd_batch_set_tiling) and, when given, the
-        member-kernel worker stream count (fdtd_batch_set_streams) and the
-        block width along k (fdtd_batch_set_block_width)."""
+        member-kernel worker stream count (fdtd_batch_set_streams), the
+        block width along k (fdtd_batch_set_block_width) and the members per
+        grouped launch (fdtd_batch_set_members_per_launch)."""
         N.check(N.lib().fdtd_batch_set_tiling(self._h, int(chunk), int(rows), int(prefetch), int(group)))
         if streams is not None:
             N.check(N.lib().fdtd_batch_set_streams(self._h, int(streams)))
         if width is not None:
             N.check(N.lib().fdtd_batch_set_block_width(self._h, int(width)))
+        if per_launch is not None:
+            N.check(N.lib().fdtd_batch_set_members_per_launch(self._h, int(per_launch)))
 
     def set_shape(self, shape: dict) -> None:
         """set_tiling from a dict as tiling() returns it ("streams" and
         "width" optional)."""
         self.set_tiling(shape["chunk"], shape["rows"], shape.get("prefetch", 1), shape.get("group", 0),
-                        shape.get("streams", 0), shape.get("width", 32))
+                        shape.get("streams", 0), shape.get("width", 32), shape.get("per_launch", 0))
 
     def tiling(self) -> dict:
-        v = [C.c_int() for _ in range(6)]
+        v = [C.c_int() for _ in range(7)]
         N.check(N.lib().fdtd_batch_get_tiling(self._h, *[C.byref(x) for x in v[:4]]))
         N.check(N.lib().fdtd_batch_get_streams(self._h, C.byref(v[4])))
         N.check(N.lib().fdtd_batch_get_block_width(self._h, C.byref(v[5])))
-        return dict(zip(("chunk", "rows", "prefetch", "group", "streams", "width"), [x.value for x in v]))
+        N.check(N.lib().fdtd_batch_get_members_per_launch(self._h, C.byref(v[6])))
+        return dict(zip(("chunk", "rows", "prefetch", "group", "streams", "width", "per_launch"),
+                        [x.value for x in v]))
 
     @property
     def cells(self) -> int:

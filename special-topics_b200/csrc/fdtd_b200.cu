@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
@@ -1795,6 +1796,13 @@ struct fdtd_batch {
   std::vector<cudaStream_t> ws;
   std::vector<cudaEvent_t> wev;
   cudaEvent_t fork_ev = nullptr;
+  // grouped mode (members_per_launch > 0, streams == 0): the members'
+  // parameter blocks travel as kernel parameters, `members_per_launch` per
+  // launch; the launches of one half-step run side by side on worker streams
+  int members_per_launch = 0;
+  std::vector<unsigned char> groups;  // host copies of the BatchGroup parameter structs
+  int ngroups = 0;
+  size_t group_size = 0;
 };
 
 namespace {
@@ -1829,6 +1837,43 @@ void (*batch_kernel(bool electric, int pf, bool persist))(const Instance<T, C>*,
   if (pf == 2) return FDTD_BK(2);
   return FDTD_BK(1);
 #undef FDTD_BK
+}
+
+// Grouped H/E kernel for a prefetch depth (as step_kernel).
+template <typename T, class C, bool EXACT>
+void (*batch_group_kernel(bool electric, int pf))(const BatchGroup<T, C>) {
+#define FDTD_GK(PF) (electric ? k_batch_group<T, C, EXACT, PF, true> : k_batch_group<T, C, EXACT, PF, false>)
+  if constexpr (C::kTable) {
+    if (pf == 3) return FDTD_GK(3);
+    if (pf == 4) return FDTD_GK(4);
+  }
+  if (pf == 2) return FDTD_GK(2);
+  return FDTD_GK(1);
+#undef FDTD_GK
+}
+
+int batch_worker_streams(fdtd_batch* b, int count);
+
+// One half-step of every group: the groups' launches fork from the batch's
+// stream onto worker streams and join back into it (also under capture).
+template <typename T, class C, bool EXACT>
+int batch_group_half(fdtd_batch* b, bool electric, size_t smem) {
+  using G = BatchGroup<T, C>;
+  auto k = batch_group_kernel<T, C, EXACT>(electric, b->prefetch);
+  const dim3 blk(b->block_w, b->block_rows);
+  CK(cudaEventRecord(b->fork_ev, b->stream));
+  for (int g = 0; g < b->ngroups; g++) {
+    const G& grp = *reinterpret_cast<const G*>(b->groups.data() + (size_t)g * sizeof(G));
+    cudaStream_t st = b->ngroups == 1 ? b->stream : b->ws[g];
+    if (st != b->stream) CK(cudaStreamWaitEvent(st, b->fork_ev, 0));
+    k<<<(unsigned)grp.first[grp.n], blk, smem, st>>>(grp);
+    if (st != b->stream) {
+      CK(cudaEventRecord(b->wev[g], st));
+      CK(cudaStreamWaitEvent(b->stream, b->wev[g], 0));
+    }
+  }
+  CK(cudaGetLastError());
+  return FDTD_OK;
 }
 
 // The parameter blocks of every member (member state may have moved since the
@@ -1866,6 +1911,41 @@ int batch_prepare(fdtd_batch* b, C (*coef_of)(fdtd_ctx*)) {
       for (long long s = 0; s < (nff * c->nFreq + 255) / 256; s++) flush.push_back(BatchBlock{q, (int)s});
   }
   if (tiles.size() > (size_t)INT32_MAX) return fail(FDTD_ERR_BADARG, "batch has too many tiles");
+  if (b->members_per_launch > 0) {
+    // grouped mode: consecutive members, members_per_launch per launch
+    using G = BatchGroup<T, C>;
+    const int per = b->members_per_launch;
+    const int ng = (n + per - 1) / per;
+    std::vector<unsigned char> gbytes((size_t)ng * sizeof(G), 0);
+    for (int g = 0; g < ng; g++) {
+      G grp;
+      memset(&grp, 0, sizeof(G));
+      grp.ts = g == 0 ? &b->d_ctl->ts : nullptr;
+      long long blocks = 0;
+      for (int q = g * per; q < std::min(n, (g + 1) * per); q++) {
+        fdtd_ctx* c = b->m[q];
+        const int k = q - g * per;
+        const int gx = (c->nz + b->block_w) / b->block_w, gy = (c->ny + b->block_rows) / b->block_rows,
+                  gz = (c->nx + 1 + b->ichunk - 1) / b->ichunk;
+        grp.first[k] = (int)blocks;
+        grp.gx[k] = gx;
+        grp.gy[k] = gy;
+        memcpy(&grp.sp[k], host.data() + (size_t)q * sizeof(In) + offsetof(In, sp), sizeof(grp.sp[k]));
+        blocks += (long long)gx * gy * gz;
+        grp.n = k + 1;
+      }
+      if (blocks > INT32_MAX) return fail(FDTD_ERR_BADARG, "batch group %d has too many blocks", g);
+      grp.first[grp.n] = (int)blocks;
+      memcpy(gbytes.data() + (size_t)g * sizeof(G), &grp, sizeof(G));
+    }
+    if (gbytes != b->groups) batch_drop_graph(b);
+    b->groups.swap(gbytes);
+    b->ngroups = ng;
+    b->group_size = sizeof(G);
+  } else {
+    b->groups.clear();
+    b->ngroups = 0;
+  }
   if (!b->d_inst || b->inst_size != sizeof(In)) {
     if (b->d_inst) cudaFree(b->d_inst);
     b->d_inst = nullptr;
@@ -1923,14 +2003,34 @@ int batch_enqueue(fdtd_batch* b, int count, KernelTimer* tm = nullptr) {
   int rc = stage_smem(kh, b->prefetch, b->block_w * b->block_rows, &smem);
   if (!rc) rc = stage_smem(ke, b->prefetch, b->block_w * b->block_rows, &smem);
   if (rc) return rc;
+  const bool grouped = b->ngroups > 0;
+  size_t gsmem = 0;
+  if (grouped) {
+    rc = batch_worker_streams(b, b->ngroups);
+    if (!rc) rc = stage_smem(batch_group_kernel<T, C, EXACT>(false, b->prefetch), b->prefetch,
+                             b->block_w * b->block_rows, &gsmem);
+    if (!rc) rc = stage_smem(batch_group_kernel<T, C, EXACT>(true, b->prefetch), b->prefetch,
+                             b->block_w * b->block_rows, &gsmem);
+    if (rc) return rc;
+  }
   for (int s = 0; s < count; s++) {
     if (tm) CK(cudaEventRecord(tm->ev[0], b->stream));
-    kh<<<gh, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    if (grouped) {
+      rc = batch_group_half<T, C, EXACT>(b, false, gsmem);
+      if (rc) return rc;
+    } else {
+      kh<<<gh, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    }
     if (tm) CK(cudaEventRecord(tm->ev[1], b->stream));
     k_batch_mid<T, C, EXACT><<<(unsigned)b->mid.size(), 256, 0, b->stream>>>(in, b->d_mid, b->d_ctl,
                                                                              (int)b->m.size());
     if (tm) CK(cudaEventRecord(tm->ev[2], b->stream));
-    ke<<<ge, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    if (grouped) {
+      rc = batch_group_half<T, C, EXACT>(b, true, gsmem);
+      if (rc) return rc;
+    } else {
+      ke<<<ge, blk, smem, b->stream>>>(in, b->d_tiles, nt, b->d_ctl, b->group);
+    }
     if (tm) CK(cudaEventRecord(tm->ev[3], b->stream));
     if (!b->epi.empty()) k_batch_epilogue<T, C><<<(unsigned)b->epi.size(), 256, 0, b->stream>>>(in, b->d_epi);
     if (!b->flush.empty())
@@ -2004,8 +2104,8 @@ struct MemberShape {
   }
 };
 
-int batch_worker_streams(fdtd_batch* b) {
-  while ((int)b->ws.size() < b->streams) {
+int batch_worker_streams(fdtd_batch* b, int count) {
+  while ((int)b->ws.size() < count) {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -2040,7 +2140,7 @@ int batch_member_enqueue(fdtd_batch* b, int count) {
 
 int batch_run_members(fdtd_batch* b, int count, float* elapsed_ms, KernelTimer* tm) {
   const int ts = b->m[0]->ts;
-  int rc = batch_worker_streams(b);
+  int rc = batch_worker_streams(b, b->streams);
   if (rc) return rc;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (elapsed_ms) {
@@ -2285,6 +2385,21 @@ int fdtd_batch_set_streams(fdtd_batch* b, int streams) {
     return fail(FDTD_ERR_BADARG, "worker streams %d outside 0..%d", streams, kMaxBatchStreams);
   if (streams != b->streams) batch_drop_graph(b);
   b->streams = streams;
+  return FDTD_OK;
+}
+
+int fdtd_batch_set_members_per_launch(fdtd_batch* b, int members) {
+  if (!b) return fail(FDTD_ERR_BADARG, "NULL batch");
+  if (members < 0 || members > kGroupMembers)
+    return fail(FDTD_ERR_BADARG, "members per launch %d outside 0..%d", members, kGroupMembers);
+  if (members != b->members_per_launch) batch_drop_graph(b);
+  b->members_per_launch = members;
+  return FDTD_OK;
+}
+
+int fdtd_batch_get_members_per_launch(const fdtd_batch* b, int* members) {
+  if (!b || !members) return fail(FDTD_ERR_BADARG, "NULL argument");
+  *members = b->members_per_launch;
   return FDTD_OK;
 }
 

@@ -95,6 +95,43 @@ __global__ void __launch_bounds__(256, MinBlocks<T, PF>::value)
   }
 }
 
+// Grouped mode: up to kGroupMembers members' parameter blocks travel as ONE
+// kernel parameter (__grid_constant__, the constant bank), so the tile code
+// reads them as it reads a single problem's parameters: no copy into shared
+// memory, and no reload after every field store, since no store can alias
+// the constant bank.  A launch covers its members' tiles back to back:
+// member m owns blocks [first[m], first[m+1]) and lays them out as its own
+// (gx x gy x gz) launch would, x fastest.
+constexpr int kGroupMembers = 22;  // 22 blocks of at most 1.4 KB + tables: inside the 32 KB parameter limit
+
+template <typename T, class C>
+struct BatchGroup {
+  int n;                         // members in this launch
+  int* ts;                       // H launch of the step's first group: advances the shared step counter
+  int first[kGroupMembers + 1];  // first block of each member, and the block count at n
+  int gx[kGroupMembers], gy[kGroupMembers];
+  StepParams<T, C> sp[kGroupMembers];
+};
+
+template <typename T, class C, bool EXACT, int PF, bool ELECTRIC>
+__global__ void __launch_bounds__(256, MinBlocks<T, PF>::value)
+    k_batch_group(const __grid_constant__ BatchGroup<T, C> g) {
+  const int b = blockIdx.x;
+  if (!ELECTRIC && g.ts && b == 0 && threadIdx.x == 0 && threadIdx.y == 0) *g.ts += 1;
+  // the member that owns this block: every operand is uniform over the block
+  int m = 0;
+#pragma unroll 1
+  while (m + 1 < g.n && b >= g.first[m + 1]) m++;
+  const int local = b - g.first[m];
+  const int gx = g.gx[m], gy = g.gy[m];
+  const int bx = local % gx, r = local / gx;
+  const int by = r % gy, bz = r / gy;
+  if (ELECTRIC)
+    step_e_tile<T, C, EXACT, PF>(g.sp[m], bx, by, bz);
+  else
+    step_h_tile<T, C, EXACT, PF>(g.sp[m], bx, by, bz);
+}
+
 // Ex(i=0) scratch planes and port currents of every instance.  Also re-arms
 // the persistent tile counters: the H launch before this one is complete and
 // the E launch after it has not started.

@@ -68,13 +68,49 @@ def test_batch_matches_solo_runs(solo, chunk, rows, pf, group, streams):
     try:
         with Batch(engs, chunk, rows, pf, group, streams) as b:
             assert b.tiling() == {"chunk": chunk, "rows": rows, "prefetch": pf, "group": group, "streams": streams,
-                                  "width": 32}
+                                  "width": 32, "per_launch": 0}
             b.run(STEPS)
             assert b.step == STEPS
         for q, e in enumerate(engs):
             assert e.step == STEPS
             assert e.status() == (0, -1)
             _assert_same(states[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+@pytest.mark.parametrize("chunk,rows,pf,width,per_launch",
+                         [(8, 4, 1, 32, 1), (3, 2, 2, 32, 3), (64, 8, 1, 16, 22), (8, 4, 3, 32, 2),
+                          (16, 16, 4, 16, 4), (5, 4, 1, 16, 3)])
+def test_grouped_batch_matches_solo_runs(solo, chunk, rows, pf, width, per_launch):
+    """Grouped mode: members' parameter blocks as kernel parameters, one
+    member per launch up to all of them in one, launches side by side."""
+    precision, states = solo
+    if pf > 2 and precision != "f32-table":
+        pytest.skip("shared-memory stages are a material-table form")
+    engs = [Engine(p, precision) for p in _members()]
+    try:
+        with Batch(engs) as b:
+            b.set_tiling(chunk, rows, pf, 0, 0, width, per_launch)
+            assert b.tiling()["per_launch"] == per_launch
+            b.run(STEPS)
+            assert b.step == STEPS
+        for q, e in enumerate(engs):
+            assert e.step == STEPS
+            assert e.status() == (0, -1)
+            _assert_same(states[q], _state(e), f"member {q}")
+    finally:
+        for e in engs:
+            e.close()
+
+
+def test_grouped_mode_rejects_too_many_members_per_launch():
+    engs = [Engine(p, "f32-table") for p in _members(8)[:2]]
+    try:
+        with Batch(engs) as b:
+            with pytest.raises(N.FdtdError):
+                b.set_tiling(8, 4, 1, 0, 0, 32, 23)
     finally:
         for e in engs:
             e.close()
@@ -193,7 +229,7 @@ def test_batch_with_time_blocked_dft_matches_solo_runs():
 
 
 def test_batch_modes_alternate_within_one_run_sequence():
-    """Tile-list and member-kernel runs of the same batch continue each other
+    """Tile-list, member-kernel and grouped runs of the same batch continue each other
     (the step counters and blocked-DFT state carry over between the modes)."""
     probs = [build_problem_from_scenario(s, 200, per_cell=False)
              for s in (small_scenario(1, "xp"), small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3)),
@@ -209,8 +245,8 @@ def test_batch_modes_alternate_within_one_run_sequence():
             b.run(30)                     # tile-list, no graph
             b.set_tiling(8, 4, 1, 0, 2)
             b.run(70)                     # member kernels: one graph replay + 6 steps
-            b.set_tiling(16, 2, 1, 0, 0)
-            b.run(64)                     # tile-list graph
+            b.set_tiling(16, 2, 1, 0, 0, 32, 2)
+            b.run(64)                     # grouped launches, one graph replay
             b.set_tiling(32, 4, 1, 0, 3)
             b.run(36)
             assert b.step == 200
