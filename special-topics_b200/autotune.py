@@ -104,7 +104,7 @@ MEMBER_SHAPES = ((32, 4, 1), (16, 4, 1), (32, 8, 1), (64, 4, 1))
 MEMBER_STEPS = 64   # member-kernel trials time whole graphs of this many steps
 # grouped mode: members per launch, then launch shapes (rows, width, prefetch) at the best count
 PER_LAUNCH = (8, 11, 16, 22)
-GROUPED_SHAPES = ((4, 32), (8, 32), (16, 32), (8, 16), (16, 16))
+GROUPED_SHAPES = ((2, 32), (4, 32), (8, 32), (8, 16), (16, 16))   # at most 256 threads a block
 
 
 def batch_key(batch) -> str:

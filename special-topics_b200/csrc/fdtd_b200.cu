@@ -80,6 +80,20 @@ struct HostIProbe {
 
 }  // namespace
 
+// CUDA graphs of whole runs, keyed by their step count.  A run of `count`
+// steps replays graphs of at most the handle's cap (kMaxGraphNodes over the
+// launches one step takes) and one of the remainder; every graph a run needs
+// is captured before the run's first launch, so no capture falls inside a
+// timed region.  A handful of counts is kept (early-stop runs advance in
+// checkpoints of a few different lengths).
+struct RunGraphs {
+  std::vector<std::pair<int, cudaGraphExec_t>> g;
+  void clear() {
+    for (auto& e : g) cudaGraphExecDestroy(e.second);
+    g.clear();
+  }
+};
+
 struct fdtd_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -130,8 +144,7 @@ struct fdtd_ctx {
   int ichunk = 1, block_rows = 8, prefetch = 1;
   int block_w = 32;   // threads of a block along k (32: a warp is one row; 16: a warp spans two rows)
   // graph cache
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
+  RunGraphs graphs;
   bool dirty = true;
   std::vector<void*> owned;  // every device allocation
   // Running digest of everything the handle was set up with: shape, spacing,
@@ -230,11 +243,7 @@ void psi_sizes(const fdtd_ctx* c, int f, int nc, long long out[4]) {
 void invalidate(fdtd_ctx* c) {
   c->dirty = true;
   c->table_dirty = true;
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-    c->graph_steps = 0;
-  }
+  c->graphs.clear();
 }
 
 template <typename T>
@@ -554,7 +563,59 @@ int close_dft_block(fdtd_ctx* c, int upto, cudaStream_t st) {
   return FDTD_OK;
 }
 
-constexpr int kGraphSteps = 64;
+constexpr int kGraphSteps = 64;       // shortest graph (and the cap's floor)
+constexpr int kMaxGraphNodes = 40000;  // kernel launches held by one graph at most
+constexpr size_t kMaxCachedGraphs = 6;
+
+// The graph of `steps` steps from the cache, captured on `st` through `enq`
+// (which enqueues that many steps) when missing.
+template <class Enq>
+int graph_for(RunGraphs& rg, cudaStream_t st, int steps, Enq enq, cudaGraphExec_t* out) {
+  for (auto& e : rg.g)
+    if (e.first == steps) {
+      *out = e.second;
+      return FDTD_OK;
+    }
+  if (rg.g.size() >= kMaxCachedGraphs) {
+    cudaGraphExecDestroy(rg.g.front().second);
+    rg.g.erase(rg.g.begin());
+  }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int erc = enq(steps);
+  cudaError_t ce = cudaStreamEndCapture(st, &g);
+  if (erc) return erc;
+  if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+  cudaGraphExec_t ge = nullptr;
+  ce = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+  rg.g.push_back({steps, ge});
+  *out = ge;
+  return FDTD_OK;
+}
+
+// The graph launches of a run of `count` steps: full graphs of `cap` steps
+// and one of the remainder, each captured (if missing) now.
+template <class Enq>
+int run_plan(RunGraphs& rg, cudaStream_t st, int count, int launches_per_step, Enq enq,
+             std::vector<cudaGraphExec_t>* plan) {
+  const int cap = std::max(kGraphSteps, kMaxGraphNodes / std::max(1, launches_per_step));
+  plan->clear();
+  if (count <= 0) return FDTD_OK;
+  cudaGraphExec_t full = nullptr, rest = nullptr;
+  if (count >= cap) {
+    int rc = graph_for(rg, st, cap, enq, &full);
+    if (rc) return rc;
+  }
+  if (count % cap) {
+    int rc = graph_for(rg, st, count % cap, enq, &rest);
+    if (rc) return rc;
+  }
+  for (int q = 0; q < count / cap; q++) plan->push_back(full);
+  if (rest) plan->push_back(rest);
+  return FDTD_OK;
+}
 
 constexpr int kMaxBatchStreams = 32;
 
@@ -572,7 +633,17 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
     rc = prepare_table(c, &c->tcoef);
     if (rc) return rc;
   }
-  int left = count;
+  // the whole run as cached graphs, captured before the first launch
+  if (c->dirty) {
+    c->graphs.clear();
+    c->dirty = false;
+  }
+  std::vector<cudaGraphExec_t> plan;
+  if (!tm) {
+    rc = run_plan(c->graphs, c->stream, count, c->dft_block > 0 ? 5 : 4,
+                  [c](int n) { return enqueue(c, n); }, &plan);
+    if (rc) return rc;
+  }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (elapsed_ms) {
     CK(cudaEventCreate(&ev0));
@@ -580,34 +651,10 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
     CK(cudaEventRecord(ev0, c->stream));
   }
   if (tm) {
-    rc = enqueue(c, left, tm);
-    if (rc) return rc;
-    left = 0;
-  }
-  // whole batches through a cached graph of kGraphSteps steps
-  while (left >= kGraphSteps) {
-    if (!c->graph || c->dirty) {
-      if (c->graph) cudaGraphExecDestroy(c->graph);
-      c->graph = nullptr;
-      cudaGraph_t g;
-      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int erc = enqueue(c, kGraphSteps);
-      cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-      if (erc) return erc;
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&c->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-      c->graph_steps = kGraphSteps;
-      c->dirty = false;
-    }
-    CK(cudaGraphLaunch(c->graph, c->stream));
-    left -= kGraphSteps;
-  }
-  if (left > 0) {
-    rc = enqueue(c, left);
+    rc = enqueue(c, count, tm);
     if (rc) return rc;
   }
+  for (cudaGraphExec_t ge : plan) CK(cudaGraphLaunch(ge, c->stream));
   if (elapsed_ms) {
     CK(cudaEventRecord(ev1, c->stream));
     CK(cudaEventSynchronize(ev1));
@@ -763,7 +810,7 @@ void fdtd_free(fdtd_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graphs.clear();
   for (void* p : c->owned) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1789,7 +1836,7 @@ struct fdtd_batch {
   std::vector<BatchBlock> mid, epi, flush;
   BatchBlock* d_flush = nullptr;
   int grid_h = 0, grid_e = 0;  // persistent grid sizes
-  cudaGraphExec_t graph = nullptr;
+  RunGraphs graphs;
   // member-kernel mode (streams > 0): each member's own step kernels, members
   // spread over `streams` worker streams joined to `stream`
   int streams = 0;
@@ -1807,10 +1854,7 @@ struct fdtd_batch {
 
 namespace {
 
-void batch_drop_graph(fdtd_batch* b) {
-  if (b->graph) cudaGraphExecDestroy(b->graph);
-  b->graph = nullptr;
-}
+void batch_drop_graph(fdtd_batch* b) { b->graphs.clear(); }
 
 template <class V>
 int upload_vec(fdtd_batch* b, V** dst, const std::vector<V>& v) {
@@ -2142,41 +2186,29 @@ int batch_run_members(fdtd_batch* b, int count, float* elapsed_ms, KernelTimer* 
   const int ts = b->m[0]->ts;
   int rc = batch_worker_streams(b, b->streams);
   if (rc) return rc;
+  // the whole run as cached graphs, captured before the first launch
+  std::vector<cudaGraphExec_t> plan;
+  if (!tm) {
+    int per_step = 0;
+    for (fdtd_ctx* c : b->m) per_step += c->dft_block > 0 ? 5 : 4;
+    rc = run_plan(b->graphs, b->stream, count, per_step, [b](int n) { return batch_member_enqueue(b, n); }, &plan);
+    if (rc) return rc;
+  }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (elapsed_ms) {
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     CK(cudaEventRecord(ev0, b->stream));
   }
-  int left = count;
   if (tm) {
     // one member at a time on the batch's stream: per-kernel times summed over members
     for (size_t q = 0; q < b->m.size() && !rc; q++) {
       MemberShape shape(b->m[q], b);
-      rc = enqueue(b->m[q], left, tm, b->stream);
+      rc = enqueue(b->m[q], count, tm, b->stream);
     }
     if (rc) return rc;
-    left = 0;
   }
-  while (left >= kGraphSteps) {
-    if (!b->graph) {
-      cudaGraph_t g;
-      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      int erc = batch_member_enqueue(b, kGraphSteps);
-      cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
-      if (erc) return erc;
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&b->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
-    }
-    CK(cudaGraphLaunch(b->graph, b->stream));
-    left -= kGraphSteps;
-  }
-  if (left > 0) {
-    rc = batch_member_enqueue(b, left);
-    if (rc) return rc;
-  }
+  for (cudaGraphExec_t ge : plan) CK(cudaGraphLaunch(ge, b->stream));
   if (elapsed_ms) {
     CK(cudaEventRecord(ev1, b->stream));
     CK(cudaEventSynchronize(ev1));
@@ -2223,37 +2255,24 @@ int batch_run(fdtd_batch* b, int count, float* elapsed_ms = nullptr, KernelTimer
   const int ctl_ts = ts - 1;
   CK(cudaMemcpyAsync(&b->d_ctl->ts, &ctl_ts, sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
+  // the whole run as cached graphs, captured before the first launch
+  std::vector<cudaGraphExec_t> plan;
+  if (!tm) {
+    const int per_step = (b->flush.empty() ? 2 : 3) + (b->ngroups > 0 ? 2 * b->ngroups : 2);
+    rc = run_plan(b->graphs, b->stream, count, per_step, [b](int n) { return batch_enqueue_any(b, n); }, &plan);
+    if (rc) return rc;
+  }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (elapsed_ms) {
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     CK(cudaEventRecord(ev0, b->stream));
   }
-  int left = count;
   if (tm) {
-    rc = batch_enqueue_any(b, left, tm);
-    if (rc) return rc;
-    left = 0;
-  }
-  while (left >= kGraphSteps) {
-    if (!b->graph) {
-      cudaGraph_t g;
-      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      int erc = batch_enqueue_any(b, kGraphSteps);
-      cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
-      if (erc) return erc;
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&b->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) return fail(FDTD_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
-    }
-    CK(cudaGraphLaunch(b->graph, b->stream));
-    left -= kGraphSteps;
-  }
-  if (left > 0) {
-    rc = batch_enqueue_any(b, left);
+    rc = batch_enqueue_any(b, count, tm);
     if (rc) return rc;
   }
+  for (cudaGraphExec_t ge : plan) CK(cudaGraphLaunch(ge, b->stream));
   if (elapsed_ms) {
     CK(cudaEventRecord(ev1, b->stream));
     CK(cudaEventSynchronize(ev1));

@@ -67,9 +67,13 @@ def test_fp64_bit_identical(case):
 
 @pytest.mark.parametrize("precision", ["f32", "f32-table"])
 def test_fp32_paths_within_tolerance(case, precision):
+    """FP32 arithmetic on the reference's loop: the x = max wall is set to the
+    reference's reads, as the oracle has it (the FP32 default wall differs
+    from the oracle by design, which the small boxes' Huygens surfaces inside
+    the CPML see within these steps)."""
     name, scn, steps, o = case
     p = build_problem_from_scenario(scn, steps)
-    with Engine(p, precision) as eng:
+    with Engine(p, precision, x_wall=False) as eng:
         eng.run(steps)
         v, vo = eng.voltages()[0], o.get("V:0")
         peak = np.abs(vo).max()
@@ -396,3 +400,23 @@ def test_block_width_validation():
         w = ctypes.c_int()
         N.check(N.lib().fdtd_ctx_get_block_width(e._h, ctypes.byref(w)))
         assert w.value == 16
+
+
+def test_whole_run_graphs_match_any_split_of_the_run():
+    """A run replays CUDA graphs of its whole length (graphs of at most the
+    handle's cap of steps plus one of the remainder, cached by step count);
+    one run of 8100 steps (past the 8000-step cap of a 5-launch step) gives
+    the same as the same steps in uneven pieces."""
+    scn = small_scenario(7, "zp", steps=8100)
+    p = build_problem_from_scenario(scn, 8100, per_cell=False)
+    with Engine(p, "f32-table", dft_block=16) as a, Engine(p, "f32-table", dft_block=16) as b:
+        a.run(8100)
+        for n in (5, 64, 1, 1000, 3030, 5, 3995):
+            b.run(n)
+        assert a.step == b.step == 8100
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        assert np.array_equal(a.currents()[0], b.currents()[0])
+        assert np.array_equal(a.field("Ez"), b.field("Ez"))
+        fa, fb = a.farfield(), b.farfield()
+        for k in FF_NAMES:
+            assert np.abs(fa[k][0] - fb[k][0]).max() <= 1e-5 * (np.abs(fa[k][0]).max() + 1e-30), k
