@@ -29,8 +29,9 @@
 //   dft(Float64Array x, dt, Float64Array freqs, shift) -> {re, im}  fdtd_dft
 //   saveState(h) -> Buffer / loadState(h, Buffer)   fdtd_ctx_state_size / save_state / load_state
 //   setDftBlock(h, steps), setDftAccumulator(h, kahan)  fdtd_ctx_set_dft_block / set_dft_accumulator
+//   setXWall(h, wall)                               fdtd_ctx_set_x_wall (E at i = nx: 0 reference reads, 1 PEC wall)
 //   batchCreate([h...]) -> b, batchRun(b, count), batchShape(b, chunk, rows, prefetch, group,
-//   streams, width), batchFree(b)                   fdtd_batch_*
+//   streams, width[, perLaunch]), batchFree(b)      fdtd_batch_*
 //
 // Built by integration/node/binding.gyp; not compiled in this repository's
 // environment, which has no Node.js (tests/test_integration_sources.py checks
@@ -252,6 +253,11 @@ Napi::Value SetDftAccumulator(const Napi::CallbackInfo& a) {
   return a.Env().Undefined();
 }
 
+Napi::Value SetXWall(const Napi::CallbackInfo& a) {
+  Check(a.Env(), fdtd_ctx_set_x_wall(Ctx(a[0]), Int(a[1])), "setXWall");
+  return a.Env().Undefined();
+}
+
 Napi::Value BatchCreate(const Napi::CallbackInfo& a) {
   Napi::Array arr = a[0].As<Napi::Array>();
   std::vector<fdtd_ctx*> hs(arr.Length());
@@ -266,13 +272,15 @@ Napi::Value BatchRun(const Napi::CallbackInfo& a) {
   return a.Env().Undefined();
 }
 
-// (b, chunk, rows, prefetch, group, streams, width): a launch shape as the
-// autotuner reports it (special-topics_b200/autotune.py, tune_batch).
+// (b, chunk, rows, prefetch, group, streams, width[, perLaunch]): a launch
+// shape as the autotuner reports it (special-topics_b200/autotune.py,
+// tune_batch); perLaunch > 0 selects grouped launches.
 Napi::Value BatchShape(const Napi::CallbackInfo& a) {
   fdtd_batch* b = Batch(a[0]);
   Check(a.Env(), fdtd_batch_set_tiling(b, Int(a[1]), Int(a[2]), Int(a[3]), Int(a[4])), "batchShape");
   Check(a.Env(), fdtd_batch_set_streams(b, Int(a[5])), "batchShape");
   Check(a.Env(), fdtd_batch_set_block_width(b, Int(a[6])), "batchShape");
+  Check(a.Env(), fdtd_batch_set_members_per_launch(b, a.Length() > 7 ? Int(a[7]) : 0), "batchShape");
   return a.Env().Undefined();
 }
 
@@ -303,6 +311,7 @@ Napi::Object Init(Napi::Env env, Napi::Object e) {
   e.Set("loadState", Napi::Function::New(env, LoadState));
   e.Set("setDftBlock", Napi::Function::New(env, SetDftBlock));
   e.Set("setDftAccumulator", Napi::Function::New(env, SetDftAccumulator));
+  e.Set("setXWall", Napi::Function::New(env, SetXWall));
   e.Set("batchCreate", Napi::Function::New(env, BatchCreate));
   e.Set("batchRun", Napi::Function::New(env, BatchRun));
   e.Set("batchShape", Napi::Function::New(env, BatchShape));
