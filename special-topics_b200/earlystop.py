@@ -391,6 +391,108 @@ def target_to_poles(y) -> list:
             for q in range(len(y) // 2)]
 
 
+# The network's target: the run's two slowest-decaying resonances inside the
+# S11 band.  These decay over thousands of steps and lie close together (a few
+# hundred MHz apart), which is what a short window of the run's own samples
+# cannot resolve; the faster poles are left to the pencils.
+N_MODES = 2
+MODE_DIM = 2 * N_MODES
+MODE_BAND = (1.0e9, 4.0e9)
+
+
+def band_modes(poles, k: int = N_MODES, band=MODE_BAND):
+    """The k slowest-decaying poles with a frequency inside `band`, slowest
+    first, or None when there are fewer."""
+    inb = [s_ for s_ in poles if band[0] <= s_.imag / (2 * math.pi) <= band[1] and s_.real < 0]
+    if len(inb) < k:
+        return None
+    return sorted(inb, key=lambda s_: s_.real, reverse=True)[:k]
+
+
+def modes_to_target(modes) -> np.ndarray:
+    y = []
+    for s_ in modes:
+        y += [(s_.imag / (2 * math.pi) - F_CENTER) / F_SCALE, math.log(-s_.real / ALPHA_UNIT)]
+    return np.array(y, np.float32)
+
+
+def target_to_modes(y) -> list:
+    return target_to_poles(y)
+
+
+def mode_label(V, I, n0: int, n1: int, dt: float, M: int = 12):
+    """Network target of a run: band_modes of a matrix pencil of order M over
+    [n0, n1) of its own traces, or None."""
+    try:
+        P = window_poles(V, I, n0, n1, dt, M=M)
+    except (ValueError, np.linalg.LinAlgError):
+        return None
+    m = band_modes(P)
+    return modes_to_target(m) if m else None
+
+
+def vp_refine(V, I, poles, n0: int, n1: int, dt: float, decim: int = DECIM, max_nfev: int = 60) -> list:
+    """Least-squares refinement of a pole set on the decimated V and I samples
+    of [n0, n1) by variable projection: the poles are the unknowns, the
+    complex amplitudes of each channel are solved for inside every residual
+    evaluation (Golub and Pereyra's separable least squares), Levenberg-
+    Marquardt from the given start.  Frequencies and log decay rates are the
+    parameters, so the poles stay decaying.  Returns the start on failure."""
+    from scipy.optimize import least_squares
+    if not poles:
+        return []
+    sv = float(np.abs(V[n0:n1]).max()) or 1.0
+    si = float(np.abs(I[n0:n1]).max()) or 1.0
+    xs = (np.asarray(V[n0:n1:decim], np.float64) / sv, np.asarray(I[n0:n1:decim], np.float64) / si)
+    t = np.arange(xs[0].size) * decim * dt
+
+    def unpack(p):
+        return [complex(-math.exp(p[2 * q + 1]) * ALPHA_UNIT, 2 * math.pi * p[2 * q] * F_SCALE)
+                for q in range(len(p) // 2)]
+
+    def res(p):
+        cols = []
+        for s_ in unpack(p):
+            e = np.exp(s_ * t)
+            cols += [e.real, -e.imag]
+        A = np.stack(cols, axis=1)
+        out = []
+        for x in xs:
+            c, *_ = np.linalg.lstsq(A, x, rcond=None)
+            out.append(x - A @ c)
+        return np.concatenate(out)
+
+    p0 = []
+    for s_ in poles:
+        p0 += [s_.imag / (2 * math.pi) / F_SCALE, math.log(max(-s_.real, 1e6) / ALPHA_UNIT)]
+    if len(p0) > 2 * xs[0].size:
+        return list(poles)
+    try:
+        r = least_squares(res, np.array(p0), method="lm", max_nfev=max_nfev * len(p0))
+    except (ValueError, np.linalg.LinAlgError):
+        return list(poles)
+    return unpack(r.x) if np.all(np.isfinite(r.x)) else list(poles)
+
+
+def vp_start(V, I, n1: int, dt: float, policy, modes=None) -> list:
+    """Start of the refinement at checkpoint n1: the given modes (the
+    network's) plus the slowest poles of the run's own pencil (order 12 over
+    [n_in, n1)) that lie more than 10% in frequency away from them, up to
+    policy.vp_poles poles in all; without modes, the pencil's slowest
+    policy.vp_poles poles."""
+    try:
+        P = window_poles(V, I, policy.n_in, n1, dt, M=12, decim=policy.decim)
+    except (ValueError, np.linalg.LinAlgError):
+        P = []
+    start = list(modes or [])
+    for s_ in sorted(P, key=lambda z: z.real, reverse=True):
+        if len(start) >= policy.vp_poles:
+            break
+        if all(abs(s_.imag - m.imag) > 0.1 * abs(m.imag) for m in (modes or [])):
+            start.append(s_)
+    return start
+
+
 def pole_tail(V, I, poles, n0: int, n_stop: int, n_total: int, dt: float):
     """Amplitudes of `poles` fitted on the steps [n0, n_stop) that were run;
     returns the traces over n_total steps (run steps, then the fitted tail)
@@ -434,6 +536,21 @@ class StopPolicy:
     n_total: int = 7000
     pencil_orders: tuple = (8, 12, 16)
     decim: int = DECIM
+    force_last: bool = True    # the last checkpoint always stops (else: plain FDTD to n_total)
+    vp: bool = False           # a refined candidate (vp_refine from vp_start) may stop a run
+    vp_poles: int = 6
+
+    @classmethod
+    def refined(cls, **kw) -> "StopPolicy":
+        """The rule the learned stop uses: checkpoints to 6000 steps, a run
+        that none of them stops finishes as plain FP32 FDTD, and at each
+        checkpoint the refined candidate (started from the network's modes, or
+        from the run's own pencil without the network) stops the run when it
+        agrees with the best-fitting pencil candidate; otherwise the pencils'
+        own agreement rule applies."""
+        base = dict(checkpoints=(2300, 3000, 4000, 5000, 6000), force_last=False, vp=True)
+        base.update(kw)
+        return cls(**base)
 
 
 def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
@@ -491,10 +608,27 @@ def s11_db_host(V, I, dt: float, freqs=None, z0: float = 50.0) -> np.ndarray:
     return postproc.s11((xv.real, xv.imag), (xi.real, xi.imag), z0)["mag_dB"]
 
 
-def stop_fit(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, last: bool = False):
+def stop_fit(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, last: bool = False, modes=None):
     """The tail (traces over n_total, residual, candidate index) a run stops
-    with at checkpoint n1, or None to keep stepping (StopPolicy's rule)."""
-    cands = tail_candidates(V, I, n1, dt, policy, net_poles)
+    with at checkpoint n1, or None to keep stepping (StopPolicy's rule).
+    With policy.vp the refined candidate (index -1) is tried first: it stops
+    the run when it and the best-fitting pencil candidate both pass the
+    residual gate and their |S11| agree within agree_db; `modes` (the
+    network's) start its refinement, else the run's own pencil does."""
+    cands = tail_candidates(V, I, n1, dt, policy, None if policy.vp else net_poles)
+    if policy.vp and cands and cands[0][2] <= policy.max_resid:
+        start = vp_start(V, I, n1, dt, policy, modes)
+        if start:
+            P = vp_refine(V, I, start, policy.n_in, n1, dt, policy.decim)
+            try:
+                v, i, r = pole_tail(V, I, P, policy.n_in, n1, policy.n_total, dt)
+            except np.linalg.LinAlgError:
+                r = float("inf")
+            if np.isfinite(r) and r <= policy.max_resid:
+                a = s11_db_host(v, i, dt)
+                b = s11_db_host(cands[0][0], cands[0][1], dt)
+                if np.abs(a - b).max() <= policy.agree_db:
+                    return v, i, r, -1
     if not cands:
         return None
     ok = [c for c in cands if c[2] <= policy.max_resid][:policy.agree_count]
@@ -509,10 +643,14 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                         use_network: bool = True) -> list[dict]:
     """Advances FP32 engines of one batch through the checkpoints of `policy`
     and stops each run at the first checkpoint where the policy's rule
-    (stop_fit) stops it; the last checkpoint always stops.  With use_network the network's pole
-    set (predicted on the device from the first n_in steps) competes with the
-    pencils.  Returns per engine {"V", "I": traces over n_total steps,
-    "stopped_at", "resid", "winner": "network" or "pencil"}."""
+    (stop_fit) stops it; with policy.force_last the last checkpoint always
+    stops, otherwise the runs left step on to n_total as plain FDTD.  With
+    use_network the network's output (predicted on the device from the first
+    n_in steps) takes part: a pole set competes with the pencils, or, for a
+    network of the two in-band modes (MODE_DIM outputs), the modes start the
+    refined candidate.  Returns per engine {"V", "I": traces over n_total
+    steps, "stopped_at", "resid", "winner": "network", "refined", "pencil" or
+    "full run"}."""
     from .backend import Batch
     out = [None] * len(engines)
     net_poles = [None] * len(engines)
@@ -536,6 +674,7 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                     y, _ = net.predict_members(sub[g0:g0 + net.max_batch], policy.decim)
                     for k, q in enumerate(active[g0:g0 + net.max_batch]):
                         net_poles[q] = target_to_poles(y[k])
+            modes_net = use_network and net is not None and net.out_dim == MODE_DIM
             traces = [(engines[q].voltages(cp)[0], engines[q].currents(cp)[0]) for q in active]
             # While the host fits this checkpoint, the GPU steps every active
             # run on to the next one (the library call releases the GIL).  The
@@ -554,7 +693,8 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
             def fit_one(k):
                 q = active[k]
                 return stop_fit(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
-                                net_poles[q] if use_network else None, last)
+                                net_poles[q] if use_network and not modes_net else None,
+                                last and policy.force_last, net_poles[q] if modes_net else None)
 
             # the fits are LAPACK-bound and release the GIL: one thread per host
             # core, each with a single BLAS thread (16 fits each spreading over
@@ -572,8 +712,9 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                 got = fits[k]
                 if got is not None:
                     v, i, r, w = got
-                    out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r,
-                              "winner": "network" if (use_network and net_poles[q] and w == 0) else "pencil"}
+                    win = ("refined" if w == -1 else
+                           "network" if (use_network and not modes_net and net_poles[q] and w == 0) else "pencil")
+                    out[q] = {"V": v, "I": i, "stopped_at": cp, "resid": r, "winner": win}
                 else:                      # keeps stepping (at the last checkpoint: to n_total)
                     rest.append(q)
             if last or not rest:

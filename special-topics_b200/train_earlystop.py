@@ -3,22 +3,24 @@
   python special-topics_b200/train_earlystop.py --out DIR [--train 4096] [--test 512] [--epochs 200]
 
 1. Transients: the batched FP32 solver runs every training variant
-   (seeds 1000..) for LABEL_END steps; the port V/I traces are kept.  (The
-   FP32 runs develop the scheme's late-time growth, a grid-scale mode seeded
-   by FP32 rounding, after about 5000 steps; labels stop before it.)
-2. Labels: the run's tail poles, a matrix pencil of order 12 over
-   [n_in, LABEL_END) of its own traces (earlystop.window_poles,
-   poles_to_target); inputs: the first n_in steps, 4x decimated and scaled
-   (earlystop.inputs_from_traces, the same values the device input builder
-   produces).
+   (seeds 1000..) for all LABEL_END = 7000 steps; the port V/I traces are
+   kept.  (FP32 problems hold the x = max wall at zero, so the runs do not
+   develop the reference's late-time growth.)
+2. Labels: the run's two slowest-decaying resonances in 1-4 GHz, from a
+   matrix pencil of order 12 over [n_in, 7000) of its own traces
+   (earlystop.mode_label); inputs: the first n_in steps, 4x decimated and
+   scaled (earlystop.inputs_from_traces, the same values the device input
+   builder produces).
 3. Training: the CUDA network (fdtd_es_train, Adam, BF16 weights) on those
    pairs, in stages of decreasing learning rate.
 4. Evaluation on held-out seeds (10000..): plain FP64 batched runs of the full
    step count give the reference S11 (301 points, 1-4 GHz) and the plain
-   time-to-S11; the FP32 runs stopped by the checkpoint rule with the
-   network's poles competing, and by the same rule with pencil poles only,
-   give theirs; plain FP32 full-length runs are reported for context.  Reported: the share of runs within 0.1 dB (max over
-   the 301 points), time-to-S11 of each method, steps run.
+   time-to-S11.  FP32 runs stopped by StopPolicy.refined(): "learned" starts
+   the refined candidate from the network's modes, "no_network" starts it
+   from the run's own pencil (the method without the network); plain FP32
+   full-length runs are reported for context.  Reported: the share of runs
+   within 0.1 dB (max over the 301 points), time-to-S11 of each method, steps
+   run.
 
 Writes DIR/es_weights.npz (EsNet.save: parameters, architecture, target
 scaling) and DIR/es_metrics.json.
@@ -52,14 +54,12 @@ def _label(args):
     V, I, n0, n1, dt = args
     _package()
     from special_topics_b200 import earlystop as ES
-    try:
-        P = ES.window_poles(V, I, n0, n1, dt, M=12)
-    except (ValueError, np.linalg.LinAlgError):
-        return None
-    return ES.poles_to_target(P) if P else None
+    return ES.mode_label(V, I, n0, n1, dt)
 
 
-LABEL_END = 4500
+# labels come from the whole run: the FP32 runs hold the x = max wall at zero
+# (fdtd_ctx_set_x_wall), so they do not develop the reference's late growth
+LABEL_END = 7000
 _T0 = time.perf_counter()
 
 
@@ -73,7 +73,6 @@ def build_set(ES, pool, seeds, steps, policy, tiling):
     V, I, dev_s = ES.run_variants(probs, LABEL_END, "f32-table", tiling=tiling, progress=log)
     log(f"training transients done ({dev_s:.1f} device s)")
     dts = [p.grid.dt for p in probs]
-    # labels from the steps before the FP32 runs' late-time growth sets in
     labels = pool.map(_label, [(V[q], I[q], policy.n_in, LABEL_END, dts[q]) for q in range(len(seeds))])
     log(f"{sum(t is not None for t in labels)} labels")
     x, y, keep = [], [], []
@@ -113,6 +112,28 @@ def plain_reference(ES, pool, seeds, policy, tiling, group=128):
         del probs, engs
         log(f"plain FP64 reference: {min(g0 + group, len(seeds))} of {len(seeds)} runs")
     return np.array(ref), t_plain
+
+
+def evaluate_plain(ES, probs, ref, tiling, traces_out, group=128):
+    """Plain FP32 runs of the full step count; their traces, dt and the FP64
+    reference S11 go to traces_out for replaying stop rules offline."""
+    from special_topics_b200.backend import Batch, Engine
+    V32, I32, dts = [], [], []
+    for g0 in range(0, len(probs), group):
+        engs = [Engine(p, "f32-table") for p in probs[g0:g0 + group]]
+        try:
+            with Batch(engs) as b:
+                if tiling:
+                    b.set_shape(tiling)
+                b.run(engs[0].problem.grid.numberOfTimeSteps)
+            for e in engs:
+                V32.append(e.voltages()[0].astype(np.float32))
+                I32.append(e.currents()[0].astype(np.float32))
+                dts.append(e.problem.grid.dt)
+        finally:
+            for e in engs:
+                e.close()
+    np.savez_compressed(traces_out, V=np.array(V32), I=np.array(I32), dt=np.array(dts), ref=ref)
 
 
 def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out=None):
@@ -189,6 +210,7 @@ def main():
     ap.add_argument("--save-test-traces", action="store_true",
                     help="also write the held-out runs' FP32 traces (es_test_traces.npz, about 110 KB per run) "
                          "for replaying stop rules offline")
+    ap.add_argument("--no-eval", action="store_true", help="train and save only")
     ap.add_argument("--shape", default="16,4,1,0,0",
                     help="batch launch shape chunk,rows,prefetch,group,streams (backend.Batch.set_tiling)")
     args = ap.parse_args()
@@ -200,7 +222,7 @@ def main():
     pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1), initializer=_package)
     _package()
     from special_topics_b200 import earlystop as ES
-    policy = ES.StopPolicy(max_resid=args.max_resid)
+    policy = ES.StopPolicy.refined(max_resid=args.max_resid)
     tiling = dict(zip(("chunk", "rows", "prefetch", "group", "streams"), (int(v) for v in args.shape.split(","))))
     metrics = {"policy": policy.__dict__, "arch": ES.ARCH}
     t0 = time.perf_counter()
@@ -223,11 +245,11 @@ def main():
     yn = (y - mu) / sd
     n_val = max(1, len(x) // 16)
     xv, yv = x[:n_val], yn[:n_val]
-    net = ES.EsNet(max_batch=512)
+    net = ES.EsNet(out_dim=y.shape[1], max_batch=512)
     net.init(args.seed)
     losses = []
     t0 = time.perf_counter()
-    w = np.ones(ES.OUT_DIM, np.float32)
+    w = np.ones(y.shape[1], np.float32)
     for stage, lr in enumerate((1e-3, 3e-4, 1e-4)):
         ep = args.epochs // 3
         losses += net.train(x[n_val:], yn[n_val:], epochs=ep, batch=args.batch, w=w, lr=lr, weight_decay=1e-4,
@@ -244,6 +266,12 @@ def main():
     log(f"trained: {metrics['training']}")
     with open(os.path.join(args.out, "es_metrics.json"), "w") as f:
         json.dump(metrics, f, indent=1)
+    if args.no_eval:
+        if args.save_test_traces:
+            evaluate_plain(ES, test_probs, ref, tiling, os.path.join(args.out, "es_test_traces.npz"))
+        pool.close()
+        net.close()
+        return
     metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling,
                                      traces_out=os.path.join(args.out, "es_test_traces.npz")
                                      if args.save_test_traces else None)

@@ -150,3 +150,37 @@ def test_growth_onset_finds_late_growth():
     assert postproc.growth_onset(decay) == -1
     on = postproc.growth_onset(decay + growth)
     assert 4000 < on < 7000
+
+
+def test_band_modes_label_round_trip():
+    poles = [complex(-3e9, 0.0), complex(-0.4e9, 2 * np.pi * 1.9e9), complex(-2.5e9, 2 * np.pi * 2.1e9),
+             complex(-0.3e9, 2 * np.pi * 5.2e9), complex(-5e9, 2 * np.pi * 0.5e9)]
+    m = ES.band_modes(poles)
+    assert m == [poles[1], poles[2]]                  # in 1-4 GHz, slowest first; 5.2 GHz and the real pole left out
+    back = ES.target_to_modes(ES.modes_to_target(m))
+    for a, b in zip(back, m):
+        assert abs(a - b) / abs(b) < 1e-6
+    assert ES.band_modes(poles[:2]) is None
+
+
+def test_refinement_recovers_close_modes_from_a_rough_start():
+    """Two resonances 180 MHz apart plus a fast one, seen only over steps
+    1500-2300: the refinement from a start 2% off in frequency (30% in
+    decay) finds the exact poles, and the refined candidate then stops the
+    run under StopPolicy.refined() with the exact tail."""
+    dt = 8.666e-13
+    m1 = ES.Mode(2.09e9, 0.45e9, 0.011 - 0.004j, 1.5e-4 + 2e-5j, 1500)
+    m2 = ES.Mode(2.27e9, 1.9e9, 0.006 + 0.002j, -6e-5 + 1e-5j, 1500)
+    m3 = ES.Mode(5.1e9, 3.0e9, 0.003 + 0.001j, 2e-5 - 1e-5j, 1500)
+    V, I = _ringing(m1, 7000, extra=m2)
+    V = V + m3.eval("V", np.arange(7000), dt)
+    I = I + m3.eval("I", np.arange(7000), dt)
+    true = [m.s() for m in (m1, m2, m3)]
+    start = [complex(s.real * 1.3, s.imag * 1.02) for s in true]
+    got = ES.vp_refine(V, I, start, 1500, 2300, dt)
+    for a, b in zip(sorted(got, key=lambda z: z.imag), true):
+        assert abs(a - b) / abs(b) < 1e-6
+    pol = ES.StopPolicy.refined(pencil_orders=(6, 6, 6), vp_poles=3)
+    fit = ES.stop_fit(V, I, 2300, dt, pol, modes=[start[0], start[1]])
+    assert fit is not None and fit[3] == -1 and fit[2] < 1e-10
+    assert np.allclose(fit[0], V, atol=1e-9) and np.allclose(fit[1], I, atol=1e-11)
