@@ -569,12 +569,13 @@ WEIGHTS = os.path.join(ROOT, "special-topics_b200", "weights", "es_ifa_variants.
 def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     """Time-to-S11 on inverted-F variants that neither training (seeds 1000..)
     nor the choice of the stop rule's thresholds (seeds 10000..10255) saw
-    (seeds 20000..): plain FP64
-    batched runs of all 7000 steps against FP32 runs stopped by the checkpoint
-    rule, with the trained network's poles competing and without them.  Each
-    time runs from the first step launch to S11 on the host (301 points,
-    1-4 GHz), the stop rule's fits and inference included, engine set-up
-    excluded."""
+    (seeds 20000..): plain FP64 batched runs of all 7000 steps, plain FP32
+    runs of all 7000 steps, and FP32 runs stopped by StopPolicy.refined()
+    with the refinement started from the trained network's modes ("learned")
+    and from the run's own pencil ("no_network", the method without the
+    network).  Each time runs from the first step launch to S11 on the host
+    (301 points, 1-4 GHz), the stop rule's fits and inference included,
+    engine set-up excluded."""
     import multiprocessing as mp
     from special_topics_b200 import earlystop as ES
     from special_topics_b200.backend import Batch, Engine
@@ -587,7 +588,7 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     # same material grids (bit-identical to the host-built arrays)
     probs64 = probs
     freqs = ES.S11_FREQS
-    policy = ES.StopPolicy()
+    policy = ES.StopPolicy.refined()
     tiling = {"chunk": 32, "rows": 4, "prefetch": 1, "group": 0}
     net = ES.EsNet.load(WEIGHTS, max_batch=max(count, 1), device=device)
     out = {"workload": f"ifa-variants-{count} (seeds {seeds[0]}..{seeds[-1]})", "steps": policy.n_total}
@@ -601,6 +602,20 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     finally:
         for e in engs:
             e.close()
+    engs = [Engine(p, "f32-table", device=device, dft_block=dft_block) for p in probs]
+    try:
+        t0 = time.perf_counter()
+        with Batch(engs) as b:
+            b.set_shape(tiling)
+            b.run(policy.n_total)
+        s11 = [ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs) for e in engs]
+        t = time.perf_counter() - t0
+    finally:
+        for e in engs:
+            e.close()
+    err = np.array([np.abs(a - b).max() for a, b in zip(s11, ref)])
+    out["plain_f32"] = {"time_s": t, "within_0p1_dB": float(np.mean(err <= 0.1)),
+                        "max_err_dB_median": float(np.median(err)), "max_err_dB_worst": float(err.max())}
     for name, use in (("learned", True), ("no_network", False)):
         engs = [Engine(p, "f32-table", device=device, dft_block=dft_block) for p in probs]
         try:
@@ -612,12 +627,15 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
             for e in engs:
                 e.close()
         err = np.array([np.abs(a - b).max() for a, b in zip(s11, ref)])
+        winners = [r["winner"] for r in res]
         out[name] = {"time_s": t, "within_0p1_dB": float(np.mean(err <= 0.1)),
                      "mean_stop_step": float(np.mean([r["stopped_at"] for r in res])),
-                     "max_err_dB_median": float(np.median(err))}
+                     "max_err_dB_median": float(np.median(err)), "max_err_dB_worst": float(err.max()),
+                     "winners": {w: winners.count(w) for w in sorted(set(winners))}}
     net.close()
     out["ratio_plain_f64_over_learned"] = out["plain_f64_s"] / out["learned"]["time_s"]
     out["ratio_plain_f64_over_no_network"] = out["plain_f64_s"] / out["no_network"]["time_s"]
+    out["ratio_plain_f64_over_plain_f32"] = out["plain_f64_s"] / out["plain_f32"]["time_s"]
     return out
 
 
