@@ -447,7 +447,8 @@ def vp_refine(V, I, poles, n0: int, n1: int, dt: float, decim: int = DECIM, max_
     t = np.arange(xs[0].size) * decim * dt
 
     def unpack(p):
-        return [complex(-math.exp(p[2 * q + 1]) * ALPHA_UNIT, 2 * math.pi * p[2 * q] * F_SCALE)
+        # log decay rates held to [-12, 6] (1/ns): a diverging step stays finite
+        return [complex(-math.exp(min(max(p[2 * q + 1], -12.0), 6.0)) * ALPHA_UNIT, 2 * math.pi * p[2 * q] * F_SCALE)
                 for q in range(len(p) // 2)]
 
     def res(p):
@@ -469,7 +470,7 @@ def vp_refine(V, I, poles, n0: int, n1: int, dt: float, decim: int = DECIM, max_
         return list(poles)
     try:
         r = least_squares(res, np.array(p0), method="lm", max_nfev=max_nfev * len(p0))
-    except (ValueError, np.linalg.LinAlgError):
+    except (ValueError, OverflowError, FloatingPointError, np.linalg.LinAlgError):
         return list(poles)
     return unpack(r.x) if np.all(np.isfinite(r.x)) else list(poles)
 
