@@ -451,17 +451,45 @@ def vp_refine(V, I, poles, n0: int, n1: int, dt: float, decim: int = DECIM, max_
         return [complex(-math.exp(min(max(p[2 * q + 1], -12.0), 6.0)) * ALPHA_UNIT, 2 * math.pi * p[2 * q] * F_SCALE)
                 for q in range(len(p) // 2)]
 
+    cache = {}
+
+    def solve(p):
+        """Basis, its QR factor, the amplitudes of both channels and the
+        residual, for the parameter vector p (kept for the Jacobian)."""
+        key = p.tobytes()
+        if key not in cache:
+            cache.clear()
+            S = np.array(unpack(p))
+            E = np.exp(np.outer(t, S))                     # n x K complex
+            A = np.empty((t.size, 2 * S.size))
+            A[:, 0::2] = E.real
+            A[:, 1::2] = -E.imag                          # Re(c e) = Re(c) Re(e) - Im(c) Im(e)
+            Q, Rm = np.linalg.qr(A)
+            cs, rs = [], []
+            for x in xs:
+                qx = Q.T @ x
+                cs.append(np.linalg.lstsq(Rm, qx, rcond=None)[0])   # a real pole leaves a zero column
+                rs.append(x - Q @ qx)
+            cache[key] = (S, E, Q, cs, np.concatenate(rs))
+        return cache[key]
+
     def res(p):
+        return solve(p)[4]
+
+    def jac(p):
+        # Kaufman's variable-projection Jacobian: -(I - Q Q^T) dA/dp c
+        S, E, Q, cs, _ = solve(p)
         cols = []
-        for s_ in unpack(p):
-            e = np.exp(s_ * t)
-            cols += [e.real, -e.imag]
-        A = np.stack(cols, axis=1)
-        out = []
-        for x in xs:
-            c, *_ = np.linalg.lstsq(A, x, rcond=None)
-            out.append(x - A @ c)
-        return np.concatenate(out)
+        for q in range(S.size):
+            ds = (2j * math.pi * F_SCALE, S[q].real)        # d s / d(freq param), d s / d(log decay)
+            for d in ds:
+                parts = []
+                for c in cs:
+                    amp = complex(c[2 * q], c[2 * q + 1])
+                    v = (amp * E[:, q] * t * d).real
+                    parts.append(-(v - Q @ (Q.T @ v)))
+                cols.append(np.concatenate(parts))
+        return np.stack(cols, axis=1)
 
     p0 = []
     for s_ in poles:
@@ -469,22 +497,25 @@ def vp_refine(V, I, poles, n0: int, n1: int, dt: float, decim: int = DECIM, max_
     if len(p0) > 2 * xs[0].size:
         return list(poles)
     try:
-        r = least_squares(res, np.array(p0), method="lm", max_nfev=max_nfev * len(p0))
+        r = least_squares(res, np.array(p0), jac=jac, method="lm", max_nfev=max_nfev * len(p0))
     except (ValueError, OverflowError, FloatingPointError, np.linalg.LinAlgError):
         return list(poles)
     return unpack(r.x) if np.all(np.isfinite(r.x)) else list(poles)
 
 
-def vp_start(V, I, n1: int, dt: float, policy, modes=None) -> list:
+def vp_start(V, I, n1: int, dt: float, policy, modes=None, pencil12=None) -> list:
     """Start of the refinement at checkpoint n1: the given modes (the
     network's) plus the slowest poles of the run's own pencil (order 12 over
-    [n_in, n1)) that lie more than 10% in frequency away from them, up to
-    policy.vp_poles poles in all; without modes, the pencil's slowest
-    policy.vp_poles poles."""
-    try:
-        P = window_poles(V, I, policy.n_in, n1, dt, M=12, decim=policy.decim)
-    except (ValueError, np.linalg.LinAlgError):
-        P = []
+    [n_in, n1), `pencil12` when already computed) that lie more than 10% in
+    frequency away from them, up to policy.vp_poles poles in all; without
+    modes, the pencil's slowest policy.vp_poles poles."""
+    if pencil12 is not None:
+        P = pencil12
+    else:
+        try:
+            P = window_poles(V, I, policy.n_in, n1, dt, M=12, decim=policy.decim)
+        except (ValueError, np.linalg.LinAlgError):
+            P = []
     start = list(modes or [])
     for s_ in sorted(P, key=lambda z: z.real, reverse=True):
         if len(start) >= policy.vp_poles:
@@ -540,6 +571,8 @@ class StopPolicy:
     force_last: bool = True    # the last checkpoint always stops (else: plain FDTD to n_total)
     vp: bool = False           # a refined candidate (vp_refine from vp_start) may stop a run
     vp_poles: int = 6
+    vp_decim: int = 16         # the refinement fits every 16th sample (modes below 8 GHz: 4.5x oversampled)
+    vp_nfev: int = 10          # residual evaluations per parameter at most
 
     @classmethod
     def refined(cls, **kw) -> "StopPolicy":
@@ -554,20 +587,26 @@ class StopPolicy:
         return cls(**base)
 
 
-def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
-    out = [list(net_poles)] if net_poles else []
+def pencil_sets(V, I, n1: int, dt: float, policy: StopPolicy, orders=None) -> list:
+    """The run's pencil pole sets over [n_in, n1), one per order (empty on failure)."""
     try:
-        sets = window_poles_orders(V, I, policy.n_in, n1, dt, policy.pencil_orders, policy.decim)
+        return window_poles_orders(V, I, policy.n_in, n1, dt, orders or policy.pencil_orders, policy.decim)
     except (ValueError, np.linalg.LinAlgError):
-        sets = []
+        return [[] for _ in (orders or policy.pencil_orders)]
+
+
+def candidate_poles(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, sets=None) -> list:
+    out = [list(net_poles)] if net_poles else []
+    if sets is None:
+        sets = pencil_sets(V, I, n1, dt, policy)
     return out + [P for P in sets if P]
 
 
-def tail_candidates(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None) -> list:
+def tail_candidates(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, sets=None) -> list:
     """(traces over n_total, residual, candidate index) of every candidate pole
     set fitted to [n_in, n1), lowest residual first."""
     out = []
-    for q, P in enumerate(candidate_poles(V, I, n1, dt, policy, net_poles)):
+    for q, P in enumerate(candidate_poles(V, I, n1, dt, policy, net_poles, sets)):
         try:
             v, i, r = pole_tail(V, I, P, policy.n_in, n1, policy.n_total, dt)
         except np.linalg.LinAlgError:
@@ -616,11 +655,14 @@ def stop_fit(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, last:
     the run when it and the best-fitting pencil candidate both pass the
     residual gate and their |S11| agree within agree_db; `modes` (the
     network's) start its refinement, else the run's own pencil does."""
-    cands = tail_candidates(V, I, n1, dt, policy, None if policy.vp else net_poles)
+    orders = tuple(policy.pencil_orders) + ((12,) if policy.vp and 12 not in policy.pencil_orders else ())
+    sets = pencil_sets(V, I, n1, dt, policy, orders)      # one SVD serves every order
+    cands = tail_candidates(V, I, n1, dt, policy, None if policy.vp else net_poles,
+                            sets[:len(policy.pencil_orders)])
     if policy.vp and cands and cands[0][2] <= policy.max_resid:
-        start = vp_start(V, I, n1, dt, policy, modes)
+        start = vp_start(V, I, n1, dt, policy, modes, sets[orders.index(12)])
         if start:
-            P = vp_refine(V, I, start, policy.n_in, n1, dt, policy.decim)
+            P = vp_refine(V, I, start, policy.n_in, n1, dt, policy.vp_decim, policy.vp_nfev)
             try:
                 v, i, r = pole_tail(V, I, P, policy.n_in, n1, policy.n_total, dt)
             except np.linalg.LinAlgError:
