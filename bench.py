@@ -570,12 +570,13 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     """Time-to-S11 on inverted-F variants that neither training (seeds 1000..)
     nor the choice of the stop rule's thresholds (seeds 10000..10255) saw
     (seeds 20000..): plain FP64 batched runs of all 7000 steps, plain FP32
-    runs of all 7000 steps, and FP32 runs stopped by StopPolicy.refined()
-    with the refinement started from the trained network's modes ("learned")
-    and from the run's own pencil ("no_network", the method without the
-    network).  Each time runs from the first step launch to S11 on the host
-    (301 points, 1-4 GHz), the stop rule's fits and inference included,
-    engine set-up excluded."""
+    runs of all 7000 steps, and FP32 runs stopped early: StopPolicy.refined()
+    with the refinement started from the trained network's modes ("learned"),
+    the same rule started from the run's own pencil ("no_network"), and the
+    pencils' agreement rule alone ("pencil_rule", StopPolicy.refined(vp=False)).
+    Each time runs from the first step launch to S11 on the host (301 points,
+    1-4 GHz), the stop rule's fits and inference included, engine set-up
+    excluded."""
     import multiprocessing as mp
     from special_topics_b200 import earlystop as ES
     from special_topics_b200.backend import Batch, Engine
@@ -616,11 +617,12 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     err = np.array([np.abs(a - b).max() for a, b in zip(s11, ref)])
     out["plain_f32"] = {"time_s": t, "within_0p1_dB": float(np.mean(err <= 0.1)),
                         "max_err_dB_median": float(np.median(err)), "max_err_dB_worst": float(err.max())}
-    for name, use in (("learned", True), ("no_network", False)):
+    for name, use, pol in (("learned", True, policy), ("no_network", False, policy),
+                           ("pencil_rule", False, ES.StopPolicy.refined(vp=False))):
         engs = [Engine(p, "f32-table", device=device, dft_block=dft_block) for p in probs]
         try:
             t0 = time.perf_counter()
-            res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use)
+            res = ES.run_with_early_stop(engs, net, pol, tiling, use_network=use)
             s11 = [ES.s11_db(r["V"], r["I"], e.problem.grid.dt, freqs) for r, e in zip(res, engs)]
             t = time.perf_counter() - t0
         finally:
@@ -636,6 +638,7 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     out["ratio_plain_f64_over_learned"] = out["plain_f64_s"] / out["learned"]["time_s"]
     out["ratio_plain_f64_over_no_network"] = out["plain_f64_s"] / out["no_network"]["time_s"]
     out["ratio_plain_f64_over_plain_f32"] = out["plain_f64_s"] / out["plain_f32"]["time_s"]
+    out["ratio_plain_f64_over_pencil_rule"] = out["plain_f64_s"] / out["pencil_rule"]["time_s"]
     return out
 
 

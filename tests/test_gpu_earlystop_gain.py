@@ -1,0 +1,98 @@
+"""What the trained network gains over the early stop without it, on inverted-F
+variants that neither training (seeds 1000..5095) nor the choice of the
+rule's thresholds (10000..10255) nor the bench (20000..) saw: 32 runs, seeds
+30000..30031.
+
+The reference is each run's plain FP64 S11 over all 7000 steps (301 points,
+1-4 GHz).  Three FP32 early stops are compared:
+  - learned:      StopPolicy.refined(), the refinement started from the
+                  shipped network's two in-band modes (predicted on the device
+                  from the first 1500 steps);
+  - pencil rule:  the pencils' agreement rule alone (vp=False), the safe rule
+                  without the network;
+  - no network:   StopPolicy.refined() started from the run's own pencil.
+Asserted: the learned rule keeps at least 31 of 32 runs within 0.1 dB, never
+stops a run later than the pencil rule, and stops at least 200 steps earlier
+on average; the network's modes lie within 5% of each run's own resonances
+(a pencil over the whole FP64 run) for at least three runs in four.  The no-network variant is
+reported, not asserted: its refined candidate starts from the pencil it is
+checked against, which makes the agreement test weak.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import load_package
+
+pkg = load_package()
+from special_topics_b200 import earlystop as ES  # noqa: E402
+from special_topics_b200.backend import Batch, Engine  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SEEDS = list(range(30000, 30032))
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "special-topics_b200",
+                       "weights", "es_ifa_variants.npz")
+TILING = {"chunk": 64, "rows": 8, "prefetch": 1, "group": 0}
+
+
+@pytest.fixture(scope="module")
+def runs():
+    probs = ES.variant_problems(SEEDS, 7000)
+    engs = [Engine(p, "f64") for p in probs]
+    try:
+        with Batch(engs) as b:
+            b.set_shape(dict(TILING, prefetch=1))
+            b.run(7000)
+        ref = [ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, ES.S11_FREQS) for e in engs]
+        labels = [ES.mode_label(e.voltages()[0], e.currents()[0], 1500, 7000, e.problem.grid.dt) for e in engs]
+    finally:
+        for e in engs:
+            e.close()
+    out = {"ref": ref, "labels": labels}
+    net = ES.EsNet.load(WEIGHTS, max_batch=len(SEEDS))
+    try:
+        assert net.out_dim == ES.MODE_DIM
+        for name, use, pol in (("learned", True, ES.StopPolicy.refined()),
+                               ("pencil_rule", False, ES.StopPolicy.refined(vp=False)),
+                               ("no_network", False, ES.StopPolicy.refined())):
+            engs = [Engine(p, "f32-table") for p in probs]
+            try:
+                res = ES.run_with_early_stop(engs, net, pol, TILING, use_network=use)
+                if name == "learned":
+                    y, _ = net.predict_members(engs)
+                    out["modes"] = [ES.target_to_modes(v) for v in y]
+            finally:
+                for e in engs:
+                    e.close()
+            err = [float(np.abs(ES.s11_db(r["V"], r["I"], p.grid.dt, ES.S11_FREQS) - f).max())
+                   for r, p, f in zip(res, probs, ref)]
+            out[name] = {"stops": np.array([r["stopped_at"] for r in res]), "err": np.array(err),
+                         "winners": [r["winner"] for r in res]}
+    finally:
+        net.close()
+    for name in ("learned", "pencil_rule", "no_network"):
+        o = out[name]
+        print(f"{name}: within 0.1 dB {np.mean(o['err'] <= 0.1):.3f}, worst {o['err'].max():.3f} dB, "
+              f"mean stop {o['stops'].mean():.0f}")
+    return out
+
+
+def test_learned_stop_is_accurate_and_earlier_than_the_rule_without_the_network(runs):
+    L, P = runs["learned"], runs["pencil_rule"]
+    assert np.sum(L["err"] <= 0.1) >= len(SEEDS) - 1
+    assert np.all(L["stops"] <= P["stops"])
+    assert P["stops"].mean() - L["stops"].mean() >= 200
+    assert "refined" in L["winners"]
+
+
+def test_network_modes_are_close_to_the_runs_resonances(runs):
+    errs = []
+    for m, y in zip(runs["modes"], runs["labels"]):
+        if y is None:
+            continue
+        t = ES.target_to_modes(y)
+        errs.append(max(abs(a.imag - b.imag) / abs(b.imag) for a, b in zip(m, t)))
+    assert len(errs) >= 24
+    assert np.mean(np.array(errs) <= 0.05) >= 0.75
