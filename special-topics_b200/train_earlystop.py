@@ -17,8 +17,9 @@
    step count give the reference S11 (301 points, 1-4 GHz) and the plain
    time-to-S11.  FP32 runs stopped by StopPolicy.refined(): "learned" starts
    the refined candidate from the network's modes, "no_network" starts it
-   from the run's own pencil (the method without the network); plain FP32
-   full-length runs are reported for context.  Reported: the share of runs
+   from the run's own pencil (the same rule without the network), and
+   "pencil_rule" is the pencils' agreement alone (the safe rule without the
+   network); plain FP32 full-length runs are reported for context.  Reported: the share of runs
    within 0.1 dB (max over the 301 points), time-to-S11 of each method, steps
    run.
 
@@ -141,13 +142,14 @@ def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out
     from special_topics_b200.backend import Batch, Engine
     freqs = ES.S11_FREQS
     out = {"plain_f64": {"time_s": t_plain, "steps": policy.n_total * len(probs)}}
-    for name, use_net in (("learned", True), ("no_network", False)):
+    for name, use_net, pol in (("learned", True, policy), ("no_network", False, policy),
+                               ("pencil_rule", False, ES.StopPolicy.refined(vp=False))):
         errs, stops, winners, t = [], [], [], 0.0
         for g0 in range(0, len(probs), group):
             engs = [Engine(p, "f32-table") for p in probs[g0:g0 + group]]
             try:
                 t0 = time.perf_counter()
-                res = ES.run_with_early_stop(engs, net, policy, tiling, use_network=use_net)
+                res = ES.run_with_early_stop(engs, net, pol, tiling, use_network=use_net)
                 s11 = [ES.s11_db(r["V"], r["I"], e.problem.grid.dt, freqs) for r, e in zip(res, engs)]
                 t += time.perf_counter() - t0
                 log(f"{name}: {g0 + len(engs)} of {len(probs)} runs")
