@@ -193,8 +193,12 @@ int fdtd_ctx_set_tiling(fdtd_ctx* ctx, int x_planes_per_thread, int block_rows);
 int fdtd_ctx_get_tiling(const fdtd_ctx* ctx, int* x_planes_per_thread, int* block_rows);
 int fdtd_ctx_set_block_width(fdtd_ctx* ctx, int threads_along_k);
 int fdtd_ctx_get_block_width(const fdtd_ctx* ctx, int* threads_along_k);
-/* How many x planes ahead the interior loop of the step kernels loads (1 or 2);
- * same results either way, chosen by the autotuner. */
+/* How the interior loop of the step kernels fetches its planes: 1 or 2 =
+ * that many planes ahead into registers; 3 or 4 (material-table problems) =
+ * that many planes staged through shared memory, word by word; 5
+ * (material-table problems, 32-wide blocks) = the H half-step's rows staged
+ * through a shared-memory ring by bulk copies on mbarriers.  Same results
+ * in every mode; the autotuner picks among 1-4. */
 int fdtd_ctx_set_prefetch(fdtd_ctx* ctx, int planes);
 /* fdtd_ctx_run that also reports the device time (ms) between CUDA events
  * recorded on the handle's stream before the first and after the last launch. */

@@ -395,6 +395,7 @@ StepParams<T, C> step_params(const fdtd_ctx* c, const C& coef) {
   p.dft_block = c->dft_block;
   p.dft_done = c->d_dft_done;
   p.x_wall = c->x_wall;
+  p.fault = c->d_status;
   return p;
 }
 
@@ -405,6 +406,7 @@ void (*step_kernel(bool electric, int pf))(StepParams<T, C>) {
   if constexpr (C::kTable) {
     if (pf == 3) return electric ? k_step_e<T, C, EXACT, 3> : k_step_h<T, C, EXACT, 3>;
     if (pf == 4) return electric ? k_step_e<T, C, EXACT, 4> : k_step_h<T, C, EXACT, 4>;
+    if (pf == 5) return electric ? k_step_e<T, C, EXACT, 5> : k_step_h<T, C, EXACT, 5>;
   }
   if (pf == 2) return electric ? k_step_e<T, C, EXACT, 2> : k_step_h<T, C, EXACT, 2>;
   return electric ? k_step_e<T, C, EXACT, 1> : k_step_h<T, C, EXACT, 1>;
@@ -414,7 +416,7 @@ void (*step_kernel(bool electric, int pf))(StepParams<T, C>) {
 // stages need more than the default 48 KB.
 template <class K>
 int stage_smem(K kernel, int pf, int threads, size_t* bytes) {
-  *bytes = pf >= 3 ? (size_t)stage_smem_bytes(pf, threads) : 0;
+  *bytes = pf == 5 ? (size_t)bulk_smem_bytes(threads) : pf >= 3 ? (size_t)stage_smem_bytes(pf, threads) : 0;
   if (*bytes > 48 * 1024)
     CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes));
   return FDTD_OK;
@@ -446,6 +448,8 @@ int enqueue_steps(fdtd_ctx* c, const C& coef, int count, KernelTimer* tm = nullp
   // a thread per (j, k) column walks `ichunk` x planes
   int rc0 = check_block(c->block_w, c->block_rows);
   if (rc0) return rc0;
+  if (c->prefetch == 5 && c->block_w != 32)
+    return fail(FDTD_ERR_BADARG, "prefetch mode 5 (bulk-copied stages) needs 32-wide blocks, got %d", c->block_w);
   const dim3 blk(c->block_w, c->block_rows);
   const dim3 grd((c->nz + c->block_w) / c->block_w, (c->ny + c->block_rows) / c->block_rows,
                  (c->nx + 1 + c->ichunk - 1) / c->ichunk);
@@ -670,6 +674,7 @@ int run_steps(fdtd_ctx* c, int count, float* elapsed_ms = nullptr, KernelTimer* 
   c->ts += count;
   int st[2];
   CK(xfer(c, st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st[0] == FDTD_ERR_CUDA) return fail(FDTD_ERR_CUDA, "a bounded device wait of the staged step ran out");
   if (st[0] != 0) return fail(FDTD_ERR_NONFINITE, "non-finite port sample at step %d", st[1]);
   return FDTD_OK;
 }
@@ -785,8 +790,10 @@ int fdtd_create(const FdtdConfig* cfg, fdtd_ctx** out) {
     for (int q = 0; q < 18 && !rc; q++) rc = dalloc(c, &c->coef[q], coef_count(c, q) * c->esz);
   }
   if (!rc && c->prec == FDTD_PREC_F32_TABLE) {
-    // 4 bytes of padding: the staged kernels copy whole aligned words of ids
-    for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6] + 4);
+    // 64 bytes of padding: the staged kernels copy whole aligned words of ids,
+    // and the bulk-copied rows (32 ids widened to 16-byte boundaries) may
+    // reach up to 47 bytes past the last id
+    for (int q = 0; q < 6 && !rc; q++) rc = dalloc(c, (void**)&c->ids[q], c->ncomp[(q + 3) % 6] + 64);
   }
   if (!rc) rc = ensure_traces(c);
   if (!rc) {
@@ -1361,9 +1368,9 @@ int fdtd_ctx_run(fdtd_ctx* c, int count) {
 
 int fdtd_ctx_set_prefetch(fdtd_ctx* c, int planes) {
   if (!c) return fail(FDTD_ERR_BADARG, "NULL handle");
-  if (planes < 1 || planes > 4) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in 1..4", planes);
+  if (planes < 1 || planes > 5) return fail(FDTD_ERR_BADARG, "prefetch depth %d not in 1..5", planes);
   if (planes > 2 && c->prec != FDTD_PREC_F32_TABLE)
-    return fail(FDTD_ERR_BADARG, "prefetch depths 3 and 4 (shared-memory stages) need a material-table problem");
+    return fail(FDTD_ERR_BADARG, "prefetch modes 3..5 (shared-memory stages) need a material-table problem");
   c->prefetch = planes;
   invalidate(c);
   return FDTD_OK;

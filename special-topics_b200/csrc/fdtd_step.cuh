@@ -164,6 +164,7 @@ struct StepParams {
   // updated and stay zero, the ranges of the MATLAB original
   // (fdtd_solve_Ch9_ex9a_12032026.m.txt:2095-2106), a PEC wall.
   int x_wall;
+  int* fault;   // the handle's status code word: 4 when a bounded wait of the bulk-staged form ran out
 };
 
 // Band of a face that contains `pos` (H: m band, E: e band): ci or -1.
@@ -708,6 +709,188 @@ __device__ __forceinline__ void h_staged_range(const StepParams<float, TableCoef
 // Bytes of dynamic shared memory the staged form needs for a block.
 __host__ __device__ constexpr int stage_smem_bytes(int S, int threads) { return S * kStageWords * threads * 4; }
 
+// ---------------------------------------------------------------------------
+// Interior planes staged by bulk copies (material-table problems, prefetch
+// mode 5, 32-wide blocks): each warp copies the rows its 32 columns read --
+// Hx, Hy, Hz, Ey(j), Ex(j), Ex(j+1), Ez(j), Ez(j+1) and the three id rows of
+// a plane -- into a ring of kBulkStages shared-memory slots with one
+// cp.async.bulk per row (lanes issue them side by side), completing on an
+// mbarrier per slot.  A row copy is widened to 16-byte boundaries (the bulk
+// copy's alignment rule) and read back from the offset of its first element.
+// The lanes then compute the plane from shared memory with the arithmetic of
+// h_store.  Waits are bounded: a wait that runs out records a fault in the
+// handle's status and the kernel carries on, so nothing hangs.
+// ---------------------------------------------------------------------------
+constexpr int kBulkStages = 4;
+constexpr int kBulkRow = 40;     // floats per staged field row (a 33-value row widened to 16 B: at most 144 B)
+constexpr int kBulkIdRow = 12;   // floats per staged id row (32 ids widened: at most 48 B)
+constexpr int kBulkRows = 8;
+constexpr int kBulkSlot = kBulkRows * kBulkRow + 3 * kBulkIdRow;  // floats per warp and stage
+constexpr int kBulkSpin = 1 << 20;                                // try_wait rounds before a wait gives up
+
+__host__ __device__ constexpr int bulk_smem_bytes(int threads) {
+  return (threads / 32) * kBulkStages * (kBulkSlot * 4 + 8);
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of a slot barrier; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (int it = 0; it < kBulkSpin; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Orders this thread's earlier shared-memory reads before later bulk (async
+// proxy) writes to the same memory.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// One row copy: `n` elements of `esz` bytes from `src`, widened to 16-byte
+// boundaries, into `dst` (16-byte aligned), completing on `bar`.  Returns the
+// bytes copied.
+__device__ __forceinline__ unsigned bulk_row(void* dst, const void* src, int n, int esz, unsigned long long* bar) {
+  const unsigned long long a = (unsigned long long)src;
+  const unsigned mis = (unsigned)(a & 15);
+  const unsigned bytes = (mis + (unsigned)(n * esz) + 15u) & ~15u;
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(a - mis), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+  return bytes;
+}
+// Offset, in elements, of the first element of a row copied from `src`.
+__device__ __forceinline__ int bulk_off(const void* src, int esz) {
+  return (int)(((unsigned long long)src & 15) / (unsigned)esz);
+}
+
+// Source of staged row t of plane i for the warp whose columns start at k0 in
+// row j (nullptr: the row does not exist there).  Rows 3 and 4 are read at
+// k + 1 too, so they hold 33 values.
+__device__ __forceinline__ const void* h_bulk_src(const StepParams<float, TableCoef>& p, int t, int i, int j, int k0) {
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1, sEx = nyp1 * nzp1;
+  const Fields<float>& f = p.f;
+  const bool jin = j < ny;
+  switch (t) {
+    case 0: return jin ? (const void*)(f.Hx + (i * sHx + j * nz + k0)) : nullptr;
+    case 1: return f.Hy + (i * sHyEz + j * nz + k0);
+    case 2: return jin ? (const void*)(f.Hz + (i * sHzEy + j * nzp1 + k0)) : nullptr;
+    case 3: return jin ? (const void*)(f.Ey + (i * sHzEy + j * nzp1 + k0)) : nullptr;
+    case 4: return f.Ex + (i * sEx + j * nzp1 + k0);
+    case 5: return jin ? (const void*)(f.Ex + (i * sEx + (j + 1) * nzp1 + k0)) : nullptr;
+    case 6: return f.Ez + (i * sHyEz + j * nz + k0);
+    case 7: return jin ? (const void*)(f.Ez + (i * sHyEz + (j + 1) * nz + k0)) : nullptr;
+    case 8: return jin ? (const void*)(p.coef.ids[0] + (i * sHx + j * nz + k0)) : nullptr;
+    case 9: return p.coef.ids[1] + (i * sHyEz + j * nz + k0);
+    default: return jin ? (const void*)(p.coef.ids[2] + (i * sHzEy + j * nzp1 + k0)) : nullptr;
+  }
+}
+
+// Staged row t of a slot: field rows first, then the three id rows.
+__device__ __forceinline__ float* bulk_row_dst(float* slot, int t) {
+  return t < kBulkRows ? slot + t * kBulkRow : slot + kBulkRows * kBulkRow + (t - kBulkRows) * kBulkIdRow;
+}
+
+// Lean planes [xa, xb) of the H columns of one warp, staged by bulk copies
+// (see above).  Every valid lane of the warp calls it together; on return
+// ez_c, ey_c hold Ez and Ey of plane xb, as after h_lean_range.
+__device__ __forceinline__ void h_bulk_range(const StepParams<float, TableCoef>& p, const HCol<float>& c, int xa,
+                                             int xb, float& ez_c, float& ey_c) {
+  if (xa >= xb) return;
+  using A = Ar<float, false>;
+  const int ny = p.g.ny, nz = p.g.nz, nyp1 = ny + 1, nzp1 = nz + 1;
+  const int sHx = ny * nz, sHyEz = nyp1 * nz, sHzEy = ny * nzp1;
+  const Fields<float>& f = p.f;
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int k0 = c.k - lane, j = c.j;
+  const unsigned mask = __activemask();
+  const int nact = __popc(mask);
+  const int nwarps = blockDim.y;
+  float* wbase = fdtd_stage_smem + w * kBulkStages * kBulkSlot;
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(fdtd_stage_smem + nwarps * kBulkStages * kBulkSlot) + w * kBulkStages;
+  if (lane == 0) {
+    for (int q = 0; q < kBulkStages; q++) mbar_init(bars + q, 1);
+    mbar_fence_init();
+  }
+  __syncwarp(mask);
+  // stage q holds plane xa + q; stage n = xb - xa (plane xb) only its Ey, Ez rows
+  const int n = xb - xa;
+  auto fill = [&](int q) {
+    float* slot = wbase + (q % kBulkStages) * kBulkSlot;
+    unsigned long long* bar = bars + q % kBulkStages;
+    unsigned bytes = 0;
+    for (int t = lane; t < kBulkRows + 3; t += nact) {
+      if (q == n && t != 3 && t != 6) continue;
+      const void* src = h_bulk_src(p, t, xa + q, j, k0);
+      if (src) bytes += bulk_row(bulk_row_dst(slot, t), src, (t == 3 || t == 4) ? 33 : 32, t < kBulkRows ? 4 : 1, bar);
+    }
+    bytes = __reduce_add_sync(mask, bytes);
+    if (lane == 0) mbar_arrive_tx(bar, bytes);
+  };
+  auto rowf = [&](int q, int t) -> const float* {
+    return bulk_row_dst(wbase + (q % kBulkStages) * kBulkSlot, t) + bulk_off(h_bulk_src(p, t, xa + q, j, k0), 4);
+  };
+  auto rowb = [&](int q, int t) -> const unsigned char* {
+    return reinterpret_cast<const unsigned char*>(bulk_row_dst(wbase + (q % kBulkStages) * kBulkSlot, t)) +
+           bulk_off(h_bulk_src(p, t, xa + q, j, k0), 1);
+  };
+  for (int q = 0; q < kBulkStages && q <= n; q++) fill(q);
+  bool ok = mbar_wait(bars, 0);
+  for (int q = 0; q < n; q++) {
+    const int i = xa + q;
+    // after a wait has run out no other is tried, so a fault costs one bound
+    if (ok) ok = mbar_wait(bars + (q + 1) % kBulkStages, ((q + 1) / kBulkStages) & 1);
+    float c0, c1, c2;
+    const float ey_i = c.hx_ok || c.hz_ok ? rowf(q, 3)[lane] : 0.f;
+    const float ez_i = rowf(q, 6)[lane];
+    if (c.hx_ok) {
+      p.coef.decode(0, rowb(q, 8)[lane], c0, c1, c2);
+      f.Hx[i * sHx + c.oa] = A::lin3(c0, rowf(q, 0)[lane], c1, A::dif(rowf(q, 3)[lane + 1], ey_i), c2,
+                                     A::dif(rowf(q, 7)[lane], ez_i));
+    }
+    const float ex = rowf(q, 4)[lane];
+    if (c.hy_ok) {
+      p.coef.decode(1, rowb(q, 9)[lane], c0, c1, c2);
+      f.Hy[i * sHyEz + c.oa] = A::lin3(c0, rowf(q, 1)[lane], c1, A::dif(rowf(q + 1, 6)[lane], ez_i), c2,
+                                       A::dif(rowf(q, 4)[lane + 1], ex));
+    }
+    if (c.hz_ok) {
+      p.coef.decode(2, rowb(q, 10)[lane], c0, c1, c2);
+      f.Hz[i * sHzEy + c.ob] = A::lin3(c0, rowf(q, 2)[lane], c1, A::dif(rowf(q, 5)[lane], ex), c2,
+                                       A::dif(rowf(q + 1, 3)[lane], ey_i));
+    }
+    __syncwarp(mask);
+    fence_proxy_async();
+    if (q + kBulkStages <= n) fill(q + kBulkStages);
+  }
+  // the carried x-neighbours for the planes after the range: Ez, Ey of plane xb
+  ez_c = c.hy_ok ? rowf(n, 6)[lane] : 0.f;
+  ey_c = c.hz_ok ? rowf(n, 3)[lane] : 0.f;
+  __syncwarp(mask);
+  if (lane == 0)   // every phase has completed: the barriers' memory may be initialised again
+    for (int q = 0; q < kBulkStages; q++)
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bars + q)) : "memory");
+  __syncwarp(mask);
+  if (!ok) atomicExch(p.fault, 4);   // the handle's status code: a device wait ran out
+}
+
 // Minimum resident 256-thread blocks per SM the register budget is fitted to:
 // FP64 values need twice the registers; a deeper register prefetch holds one
 // more plane; the shared-memory stages (PF 3, 4) hold theirs outside registers.
@@ -721,9 +904,11 @@ struct MinBlocks {
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void h_lean_range(const StepParams<T, C>& p, const HCol<T>& c, int xa, int xb, T& ez_c,
                                              T& ey_c) {
-  if constexpr (PF >= 3 && C::kTable) {
+  if constexpr (PF == 5 && C::kTable) {
+    h_bulk_range(p, c, xa, xb, ez_c, ey_c);
+  } else if constexpr (PF >= 3 && PF <= 4 && C::kTable) {
     h_staged_range<PF>(p, c, xa, xb, ez_c, ey_c);
-  } else if (PF == 1 && xa < xb) {
+  } else if ((PF == 1 || PF == 5) && xa < xb) {
     // software pipeline, depth 1, as two alternating register sets: the next
     // plane's loads are in flight while plane i is computed and stored, and
     // no set is copied into the other
@@ -1287,9 +1472,9 @@ __device__ __forceinline__ void e_staged_range(const StepParams<float, TableCoef
 template <typename T, class C, bool EXACT, int PF>
 __device__ __forceinline__ void e_lean_range(const StepParams<T, C>& p, const ECol<T>& c, int xa, int xb, T& hz_p,
                                              T& hy_p) {
-  if constexpr (PF >= 3 && C::kTable) {
+  if constexpr (PF >= 3 && PF <= 4 && C::kTable) {
     e_staged_range<PF>(p, c, xa, xb, hz_p, hy_p);
-  } else if (PF == 1 && xa < xb) {
+  } else if ((PF == 1 || PF == 5) && xa < xb) {
     // depth 1 as two alternating register sets (see h_lean_range)
     EIn<T, C> a, b;
     e_load(p, c, xa, a);

@@ -310,6 +310,39 @@ def test_shared_memory_stages_give_identical_table_results(chunk, rows, pf, widt
             autotune.set_tiling(c, 8, 4, 3)
 
 
+@pytest.mark.parametrize("case_name,steps", [("ifa-fr4-substrate", 120), ("small-yn", 60), ("box-64", 80)])
+@pytest.mark.parametrize("chunk,rows", [(8, 4), (1, 2), (5, 8), (64, 1), (16, 4)])
+def test_bulk_staged_form_gives_identical_table_results(case_name, steps, chunk, rows):
+    """Prefetch mode 5 stages each warp's interior rows through shared memory
+    with bulk copies on an mbarrier ring; the results are bit-identical to
+    the depth-1 register form, for every chunk and block height, including
+    warps cut short at the k end and chunks shorter than the ring."""
+    from special_topics_b200 import autotune, workloads
+    if case_name == "box-64":
+        scn = workloads.scaling_box((64, 64, 64), seed=3, steps=steps)
+    elif case_name == "small-yn":
+        scn = small_scenario(2, "yn", ncpml=(3, 3, 5, 4, 6, 3), steps=steps)
+    else:
+        scn = load_scenario(case_name)
+    p = build_problem_from_scenario(scn, steps, per_cell=False)
+    with Engine(p, "f32-table") as a, Engine(p, "f32-table") as b:
+        autotune.set_tiling(a, 8, 4, 1)
+        autotune.set_tiling(b, min(chunk, p.grid.nx + 1), rows, 5)
+        a.run(steps)
+        b.run(steps)
+        assert b.status() == (0, -1)
+        assert np.array_equal(a.voltages()[0], b.voltages()[0])
+        for fld in ("Hx", "Hy", "Hz", "Ex", "Ey", "Ez"):
+            assert np.array_equal(a.field(fld), b.field(fld)), fld
+        fa, fb = a.farfield(), b.farfield()
+        for k in FF_NAMES:
+            assert np.array_equal(fa[k][0], fb[k][0]), k
+    with Engine(p, "f32-table") as c:
+        autotune.set_tiling(c, 8, 4, 5, 16)
+        with pytest.raises(N.FdtdError):
+            c.run(2)
+
+
 @pytest.mark.parametrize("precision", ["f64", "f32-table"])
 def test_state_checkpoint_resumes_bit_identically(precision):
     scn, steps = CASES["small-zp"]()
