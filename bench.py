@@ -329,20 +329,24 @@ def main():
     t0 = time.perf_counter()
     if not args.no_e2e:
         eng = Engine(prob, args.precision, device=local, dft_block=dft_block)
+        t_up = time.perf_counter()
         if tuning:
             autotune.set_tiling(eng, tuning["chunk"], tuning["rows"], tuning.get("prefetch", 1), tuning.get("width", 32))
         h2d = _uploaded_bytes(prob, args.precision)
         eng.run(K)
+        t_run = time.perf_counter()
         V, I = eng.voltages(K), eng.currents(K)
         ff = eng.farfield()
         e2e_s = time.perf_counter() - t0
+        e2e_parts = {"create_and_upload_s": t_up - t0, "run_s": t_run - t_up, "readback_s": e2e_s - (t_run - t0)}
         d2h = sum(v.nbytes for v in V + I) + sum(a[0].nbytes + a[1].nbytes for a in ff.values())
         eng.close()
         e2e_s = max_over_ranks(e2e_s)
         e2e = {"value": world * cells * K / e2e_s / 1e9, "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                "note": "one step's share of a whole run through the C ABI: uploads from host buffers, "
-                       "K steps, readback of port traces and far-field accumulators"}
+                       "K steps, readback of port traces and far-field accumulators",
+               "parts_rank0": e2e_parts}
 
     # --- device-timed run
     eng = Engine(prob, args.precision, device=local, dft_block=dft_block)
