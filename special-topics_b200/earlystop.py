@@ -576,15 +576,14 @@ class StopPolicy:
 
     @classmethod
     def refined(cls, **kw) -> "StopPolicy":
-        """The rule the learned stop uses: checkpoints every 400-500 steps
-        from 2300 to 6500, a run that none of them stops finishes as plain
+        """The rule the learned stop uses: checkpoints at 2300, 3000, 4000,
+        5000 and 6000 steps, a run that none of them stops finishes as plain
         FP32 FDTD, and at each
         checkpoint the refined candidate (started from the network's modes, or
         from the run's own pencil without the network) stops the run when it
         agrees with the best-fitting pencil candidate; otherwise the pencils'
         own agreement rule applies."""
-        base = dict(checkpoints=(2300, 2700, 3100, 3500, 4000, 4500, 5000, 5500, 6000, 6500), force_last=False,
-                    vp=True)
+        base = dict(checkpoints=(2300, 3000, 4000, 5000, 6000), force_last=False, vp=True)
         base.update(kw)
         return cls(**base)
 
