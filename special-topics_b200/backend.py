@@ -208,7 +208,7 @@ class Engine:
         out = {}
         for a, name in enumerate(FF_NAMES):
             n = ff.nFreq * sizes[(a % 12) // 4]
-            re, im = np.zeros(n), np.zeros(n)
+            re, im = np.empty(n), np.empty(n)      # every value is overwritten
             N.check(N.lib().fdtd_ctx_read_farfield(self._h, a, N.dptr(re), N.dptr(im), n))
             out[name] = (re, im)
         return out
