@@ -591,11 +591,11 @@ __device__ __forceinline__ void h_band_range(const StepParams<T, C>& p, const HC
   }
 }
 
-// The band form is used for material-table problems; the per-cell layouts
-// (FP64 drop-in) keep the plane-at-a-time form, which needs fewer registers.
+// The band form (all loads of a band plane issued before its stores) serves
+// every coefficient layout whose CPML bands are disjoint per axis.
 template <class C>
 struct BandForm {
-  static constexpr bool kUse = C::kTable;
+  static constexpr bool kUse = true;
   static constexpr bool kPrefetch = false;
 };
 
