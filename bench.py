@@ -594,13 +594,15 @@ def time_to_s11_side(count: int, device: int = 0, dft_block: int = 0) -> dict:
     probs64 = probs
     freqs = ES.S11_FREQS
     policy = ES.StopPolicy.refined()
-    tiling = {"chunk": 32, "rows": 4, "prefetch": 1, "group": 0}
+    # the batch tuner's shape for the inverted-F variants: one x chunk per column, 16-wide blocks
+    tiling = {"chunk": 64, "rows": 16, "prefetch": 1, "group": 0, "width": 16}
     net = ES.EsNet.load(WEIGHTS, max_batch=max(count, 1), device=device)
     out = {"workload": f"ifa-variants-{count} (seeds {seeds[0]}..{seeds[-1]})", "steps": policy.n_total}
     engs = [Engine(p, "f64", device=device) for p in probs64]
     try:
         t0 = time.perf_counter()
         with Batch(engs) as b:
+            b.set_shape(tiling)            # every method runs the same launch shape
             b.run(policy.n_total)
         ref = [ES.s11_db(e.voltages()[0], e.currents()[0], e.problem.grid.dt, freqs) for e in engs]
         out["plain_f64_s"] = time.perf_counter() - t0
