@@ -683,6 +683,42 @@ def stop_fit(V, I, n1: int, dt: float, policy: StopPolicy, net_poles=None, last:
     return cands[0] if last else None
 
 
+def _warm_worker(i: int) -> int:
+    return i
+
+
+def _fit_job(job):
+    V, I, cp, dt, policy, net_poles, last, modes = job
+    return stop_fit(V, I, cp, dt, policy, net_poles, last, modes)
+
+
+_FIT_POOL = None
+_FIT_WORKERS = 1
+
+
+def start_fit_pool(workers: int | None = None) -> None:
+    """Starts the process pool the refined rule's checkpoint fits run in (spawned,
+    so it is safe after CUDA is initialised; kept for the life of the process).
+    Without it the fits run in threads of this process."""
+    global _FIT_POOL, _FIT_WORKERS
+    if _FIT_POOL is not None:
+        return
+    import multiprocessing as mp
+    import runpy
+    _FIT_WORKERS = workers or min(16, os.cpu_count() or 1)
+    boot = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_fit_worker.py")
+    _FIT_POOL = mp.get_context("spawn").Pool(_FIT_WORKERS, initializer=runpy.run_path, initargs=(boot,))
+    _FIT_POOL.map(_warm_worker, range(_FIT_WORKERS), chunksize=1)   # every worker imports its modules now
+
+
+def stop_fit_pool() -> None:
+    global _FIT_POOL
+    if _FIT_POOL is not None:
+        _FIT_POOL.close()
+        _FIT_POOL.join()
+        _FIT_POOL = None
+
+
 def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: dict | None = None,
                         use_network: bool = True) -> list[dict]:
     """Advances FP32 engines of one batch through the checkpoints of `policy`
@@ -734,18 +770,21 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                 ahead = threading.Thread(target=step_ahead)
                 ahead.start()
 
-            def fit_one(k):
-                q = active[k]
-                return stop_fit(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
-                                net_poles[q] if use_network and not modes_net else None,
-                                last and policy.force_last, net_poles[q] if modes_net else None)
-
-            # the fits are LAPACK-bound and release the GIL: one thread per host
-            # core, each with a single BLAS thread (16 fits each spreading over
-            # every core oversubscribe the host many times over)
+            jobs = [(traces[k][0], traces[k][1], cp, engines[q].problem.grid.dt, policy,
+                     net_poles[q] if use_network and not modes_net else None, last and policy.force_last,
+                     net_poles[q] if modes_net else None) for k, q in enumerate(active)]
             try:
-                with threadpool_limits(limits=1), ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
-                    fits = list(ex.map(fit_one, range(len(active))))
+                pool = _FIT_POOL if policy.vp else None
+                if pool is not None:
+                    # the refinement's Levenberg-Marquardt loop is Python: worker
+                    # processes (one BLAS thread each) run the fits side by side
+                    fits = pool.map(_fit_job, jobs, chunksize=max(1, len(jobs) // (4 * _FIT_WORKERS)))
+                else:
+                    # LAPACK-bound fits release the GIL: one thread per host core,
+                    # each with a single BLAS thread
+                    with threadpool_limits(limits=1), \
+                            ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+                        fits = list(ex.map(lambda j: _fit_job(j), jobs))
             finally:
                 if ahead is not None:
                     ahead.join()

@@ -184,3 +184,25 @@ def test_refinement_recovers_close_modes_from_a_rough_start():
     fit = ES.stop_fit(V, I, 2300, dt, pol, modes=[start[0], start[1]])
     assert fit is not None and fit[3] == -1 and fit[2] < 1e-10
     assert np.allclose(fit[0], V, atol=1e-9) and np.allclose(fit[1], I, atol=1e-11)
+
+
+def test_fit_pool_gives_the_in_process_fits():
+    """The refined rule's checkpoint fits in the spawned worker pool give what
+    the same fits give in this process."""
+    dt = 8.666e-13
+    m1 = ES.Mode(2.09e9, 0.45e9, 0.011 - 0.004j, 1.5e-4 + 2e-5j, 1500)
+    m2 = ES.Mode(2.27e9, 1.9e9, 0.006 + 0.002j, -6e-5 + 1e-5j, 1500)
+    V, I = _ringing(m1, 7000, extra=m2)
+    pol = ES.StopPolicy.refined(pencil_orders=(4, 4, 4), vp_poles=2)
+    modes = [complex(m1.s().real * 1.2, m1.s().imag * 1.01), complex(m2.s().real * 0.8, m2.s().imag * 0.99)]
+    jobs = [(V[:cp], I[:cp], cp, dt, pol, None, False, modes) for cp in (2300, 3000)]
+    ES.start_fit_pool(2)
+    try:
+        got = ES._FIT_POOL.map(ES._fit_job, jobs)
+    finally:
+        ES.stop_fit_pool()
+    for job, g in zip(jobs, got):
+        want = ES._fit_job(job)
+        assert (g is None) == (want is None)
+        if want is not None:
+            assert g[3] == want[3] and np.array_equal(g[0], want[0]) and g[2] == want[2]
