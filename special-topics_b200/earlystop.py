@@ -694,6 +694,9 @@ def _fit_job(job):
 
 _FIT_POOL = None
 _FIT_WORKERS = 1
+# steps of one run of the step-ahead during a checkpoint's fits: a multiple of
+# the far-field DFT's time block, short against the fits' duration
+AHEAD_STEPS = 48
 
 
 def start_fit_pool(workers: int | None = None) -> None:
@@ -745,9 +748,10 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
 
     b = batch_of(active)
     try:
-        b.run(cps[0] - b.step)
         for n, cp in enumerate(cps):
             last = n == len(cps) - 1
+            if b.step < cp:
+                b.run(cp - b.step)
             if use_network and net is not None and n == 0:
                 sub = [engines[q] for q in active]
                 for g0 in range(0, len(sub), net.max_batch):
@@ -757,14 +761,17 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
             modes_net = use_network and net is not None and net.out_dim == MODE_DIM
             traces = [(engines[q].voltages(cp)[0], engines[q].currents(cp)[0]) for q in active]
             # While the host fits this checkpoint, the GPU steps every active
-            # run on to the next one (the library call releases the GIL).  The
+            # run on towards the next one (the library call releases the GIL),
+            # in short runs so that it stops soon after the fits return: the
             # runs that stop here are stepped for nothing, which costs less
-            # than leaving the GPU idle during the fits.
-            ahead, err = None, []
+            # than leaving the GPU idle during the fits, but only while the
+            # fits last.
+            ahead, err, fitted = None, [], threading.Event()
             if not last:
-                def step_ahead(bt=b, count=cps[n + 1] - cp):
+                def step_ahead(bt=b, target=cps[n + 1]):
                     try:
-                        bt.run(count)
+                        while not fitted.is_set() and bt.step < target:
+                            bt.run(min(AHEAD_STEPS, target - bt.step))
                     except Exception as e:  # re-raised on this thread after the fits
                         err.append(e)
                 ahead = threading.Thread(target=step_ahead)
@@ -786,6 +793,7 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                             ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
                         fits = list(ex.map(lambda j: _fit_job(j), jobs))
             finally:
+                fitted.set()
                 if ahead is not None:
                     ahead.join()
             if err:
@@ -802,7 +810,7 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                     rest.append(q)
             if last or not rest:
                 break
-            if len(rest) != len(active):   # the rest are at the next checkpoint already
+            if len(rest) != len(active):   # the rest step on from where the step-ahead left them
                 b.close()
                 b = batch_of(rest)
             active = rest

@@ -52,6 +52,7 @@ def runs():
             e.close()
     out = {"ref": ref, "labels": labels}
     net = ES.EsNet.load(WEIGHTS, max_batch=len(SEEDS))
+    ES.start_fit_pool()            # the checkpoint fits in worker processes, as the bench runs them
     try:
         assert net.out_dim == ES.MODE_DIM
         for name, use, pol in (("learned", True, ES.StopPolicy.refined()),
@@ -72,6 +73,7 @@ def runs():
                          "winners": [r["winner"] for r in res]}
     finally:
         net.close()
+        ES.stop_fit_pool()
     for name in ("learned", "pencil_rule", "no_network"):
         o = out[name]
         print(f"{name}: within 0.1 dB {np.mean(o['err'] <= 0.1):.3f}, worst {o['err'].max():.3f} dB, "
