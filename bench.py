@@ -298,9 +298,9 @@ def main():
         vsteps = 2 * args.warmup + args.batch_steps + 16 + _at.batch_steps_needed(args.tune_steps)
         seeds = list(range(args.batch_members))
         if world > 1:
-            seeds = [seeds[q] for q in sharding.partition(sharding.variant_costs(seeds, 7000), world)[rank]]
+            seeds = [seeds[q] for q in sharding.partition(sharding.variant_costs(seeds, 7000, True), world)[rank]]
         with mp.get_context("spawn").Pool(max(1, min(16, (os.cpu_count() or 1) // world))) as pool:
-            variants = variant_problems(seeds, max(7000, vsteps), pool)
+            variants = variant_problems(seeds, max(7000, vsteps), pool, spread=True)
 
     K, W, P = args.steps, args.warmup, 16
     dft_block = args.dft_block if args.precision != "f64" else 0   # FP64 keeps the reference's per-step sums
@@ -455,17 +455,20 @@ def _uploaded_bytes(p, precision: str) -> int:
 
 
 def _variant_problem(args):
-    seed, steps = args
+    seed, steps, spread = args
     pkg = _package()
     from special_topics_b200 import workloads
     from special_topics_b200.scenario import build_problem_from_scenario
-    return build_problem_from_scenario(workloads.ifa_variant(seed, steps=steps), steps, per_cell=False)
+    return build_problem_from_scenario(workloads.ifa_variant(seed, steps=steps, spread=spread), steps,
+                                      per_cell=False)
 
 
-def variant_problems(seeds, steps: int, pool=None) -> list:
-    """The batched-sweep members (inverted-F variants of the given seeds)."""
+def variant_problems(seeds, steps: int, pool=None, spread: bool = False) -> list:
+    """Inverted-F variants of the given seeds (workloads.ifa_variant): the
+    batched sweep's members with spread=True (grids spanning 32x96x96 ..
+    64x200x200), the time-to-S11 runs without."""
     _package()    # results unpickle into the package's classes
-    jobs = [(int(s), steps) for s in seeds]
+    jobs = [(int(s), steps, spread) for s in seeds]
     if pool is None:
         return [_variant_problem(j) for j in jobs]
     return pool.map(_variant_problem, jobs)
@@ -548,7 +551,10 @@ def batched_side(problems, K: int = 1000, W: int = 8, tune_steps: int = 16, devi
         roof_bytes, roof_ms = byts[dom], kern[dom]
     ach = roof_bytes / (roof_ms / 1e3) / 1e9
     dims = [(p.grid.nx, p.grid.ny, p.grid.nz) for p in problems]
-    return {"workload": f"ifa-variants-{len(problems)}", "members": len(problems), "cells": cells,
+    span = np.array(dims)
+    return {"workload": f"ifa-variants-{len(problems)} (grids drawn from 32x96x96 .. 64x200x200)",
+            "members": len(problems), "cells": cells,
+            "grid_span_per_axis": [[int(a), int(b)] for a, b in zip(span.min(0), span.max(0))],
             "far_field_dft": f"time-blocked, {dft_block} steps per block" if dft_block else "every step",
             "grid_min": list(min(dims, key=lambda d: d[0] * d[1] * d[2])),
             "grid_max": list(max(dims, key=lambda d: d[0] * d[1] * d[2])),

@@ -35,13 +35,14 @@ def imbalance(costs, parts) -> float:
     return max(loads) / mean if mean else 1.0
 
 
-def variant_costs(seeds, steps: int) -> list[int]:
-    """cells x steps of each inverted-F variant, from its grid alone."""
+def variant_costs(seeds, steps: int, spread: bool = False) -> list[int]:
+    """cells x steps of each inverted-F variant (workloads.ifa_variant with
+    `spread`), from its grid alone."""
     from .scenario import DEFAULTS, build_grid
     from .workloads import ifa_variant
     out = []
     for s in seeds:
-        scn = ifa_variant(int(s), steps=steps)
+        scn = ifa_variant(int(s), steps=steps, spread=spread)
         cell = dict(DEFAULTS["cell"], **(scn.get("cell") or {}))
         g = build_grid(cell["dx"], cell["dy"], cell["dz"], scn["boundary"], scn.get("bricks") or [],
                        scn.get("spheres") or [], scn.get("courantFactor", DEFAULTS["courantFactor"]), steps)

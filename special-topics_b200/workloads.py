@@ -14,7 +14,9 @@ schema (js_fdtd/scenarios/*.json, read by scenario.py like scenario.js reads it)
                      cells) and a PEC half-wave dipole with a 50-ohm gap source,
                      1 mm cells, 8-cell CPML.
   ifa_variant(seed)  one member of the batched sweep: arm U[20,35] mm, stub-to-feed
-                     U[2,8] mm, substrate eps_r U[2.2,6.15], thickness U[0.8,3.2] mm.
+                     U[2,8] mm, substrate eps_r U[2.2,6.15], thickness U[0.8,3.2] mm;
+                     spread=True pads it with air to grid extents drawn from
+                     32x96x96 .. 64x200x200.
 
 All inputs are synthetic; nothing here is data from the reference.
 """
@@ -99,8 +101,18 @@ def ifa_config2(steps: int = 20000) -> dict:
     return s
 
 
-def ifa_variant(seed: int, steps: int = 7000) -> dict:
-    """A batched-sweep member; the cell size keeps the grid inside 32x96x96 .. 64x200x200."""
+VARIANT_SPAN = ((32, 64), (96, 200), (96, 200))   # grid extents of the batched sweep, cells
+SPREAD_MIN_AIR = 6                                 # air cells per face of a spread variant, at least
+
+
+def ifa_variant(seed: int, steps: int = 7000, spread: bool = False) -> dict:
+    """A batched-sweep member on 0.5 mm cells with 8-cell CPML.  The antenna
+    alone (10 air cells per face) gives grids of 39x117x107 .. 42x146x136.
+    spread=True keeps the same antenna and draws the grid's extent along each
+    axis uniformly from VARIANT_SPAN (a second random stream of the seed;
+    never below the antenna plus SPREAD_MIN_AIR air cells per face), padding
+    with air: the members then span 32x96x96 .. 64x200x200 as far as the
+    antennas fit."""
     rng = np.random.default_rng(seed)
     arm = rng.uniform(20, 35) * MM
     stub = rng.uniform(2, 8) * MM
@@ -109,8 +121,20 @@ def ifa_variant(seed: int, steps: int = 7000) -> dict:
     cell = 0.5 * MM
     hc = max(1, round(h / cell)) * cell
     board = (round((arm + 20 * MM) / cell) * cell, round((arm + 15 * MM) / cell) * cell)
-    return _ifa(cell, hc, eps, round(arm / cell) * cell, stub, board=board, steps=steps, ncpw=60,
-                name=f"ifa-variant-{seed}")
+    scn = _ifa(cell, hc, eps, round(arm / cell) * cell, stub, board=board, steps=steps, ncpw=60,
+               name=f"ifa-variant-{seed}")
+    if spread:
+        ncpml = scn["boundary"]["cpml_cells_xn"]
+        body = (round(hc / cell), round(board[0] / cell), round(board[1] / cell))   # the bricks' extent, cells
+        grng = np.random.default_rng([seed, 1])
+        for ax, n0, (lo, hi) in zip("xyz", body, VARIANT_SPAN):
+            least = n0 + 2 * (ncpml + SPREAD_MIN_AIR)
+            n = max(int(grng.integers(lo, hi + 1)), least)
+            air = n - n0 - 2 * ncpml
+            scn["boundary"][f"air_buffer_{ax}n"] = air // 2
+            scn["boundary"][f"air_buffer_{ax}p"] = air - air // 2
+        scn["name"] = f"ifa-variant-spread-{seed}"
+    return scn
 
 
 def scaling_box(n=(128, 128, 128), seed: int = 1, cell: float = 1 * MM, ncpml: int = 8, air: int = 4,

@@ -31,6 +31,31 @@ def test_partition_covers_every_problem_once_and_balances():
 def test_variant_costs_follow_the_grids():
     c = sharding.variant_costs([0, 9], 7000)
     assert c[0] == 38 * 135 * 125 * 7000 and c[1] == 41 * 142 * 132 * 7000
+    c = sharding.variant_costs([0], 7000, spread=True)
+    assert c[0] == 49 * 189 * 200 * 7000
+
+
+def test_spread_variants_span_the_sweep_range_with_the_same_antennas():
+    """The batched sweep's members (spread=True) keep each seed's antenna and
+    fill grids drawn from 32x96x96 .. 64x200x200: extents inside that range,
+    its x ends reached, every face at least SPREAD_MIN_AIR air cells."""
+    from special_topics_b200 import workloads as W
+    from special_topics_b200.scenario import DEFAULTS, build_grid
+    dims = []
+    for seed in range(128):
+        a, b = W.ifa_variant(seed), W.ifa_variant(seed, spread=True)
+        assert a["bricks"] == b["bricks"] and a["voltageSources"] == b["voltageSources"]
+        assert a["materialTypes"] == b["materialTypes"]
+        bd = b["boundary"]
+        assert min(bd[f"air_buffer_{f}"] for f in ("xn", "xp", "yn", "yp", "zn", "zp")) >= W.SPREAD_MIN_AIR
+        cell = dict(DEFAULTS["cell"], **b["cell"])
+        g = build_grid(cell["dx"], cell["dy"], cell["dz"], bd, b["bricks"], [], 0.9, 10)
+        dims.append((g.nx, g.ny, g.nz))
+    d = np.array(dims)
+    for ax, (lo, hi) in enumerate(W.VARIANT_SPAN):
+        assert d[:, ax].min() >= lo and d[:, ax].max() <= hi
+    assert d[:, 0].min() == 32 and d[:, 0].max() == 64
+    assert d[:, 1].max() >= 195 and d[:, 2].max() >= 195
 
 
 def _rank(rank, world, port, seeds, out):
