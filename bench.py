@@ -686,7 +686,8 @@ def _leg(p, precision: str, K: int, W: int, tiling: dict | None, device: int = 0
 
 def scaling_sweep_side(tiling32: dict | None, tiling64: dict | None, device: int = 0, dft_block: int = 0,
                        grids=SWEEP_GRIDS) -> list:
-    """configs[1] at every size in FP32 material tables and FP64 (per-cell
+    """The scaling boxes (128^3, 256^3, 384^3, 512x512x640; 32 dielectric
+    blocks and a dipole) at every size in FP32 material tables and FP64 (per-cell
     coefficients built on the device, bit-identical to the host-built ones).
     About 2 G cell-updates are timed per leg (at least 20 steps).  Grids whose
     FP32 working set fits the 126 MB L2 are marked L2-resident: their rate is
@@ -711,7 +712,7 @@ def scaling_sweep_side(tiling32: dict | None, tiling64: dict | None, device: int
 
 
 def config0_side(device: int = 0, oracle_steps: int = 1000) -> dict:
-    """The north_star's parity scenario: the 0.5 mm inverted-F antenna (39 x 136
+    """The FP64 parity scenario: the 0.5 mm inverted-F antenna (39 x 136
     x 136, 7000 steps, far field at 2.4 GHz).  Device-timed FP64 (the drop-in)
     and FP32-table runs of the whole 7000 steps; time-to-S11 (301 points,
     1-4 GHz) from the first step launch to S11 on the host for each; the CPU
