@@ -697,6 +697,8 @@ _FIT_WORKERS = 1
 # steps of one run of the step-ahead during a checkpoint's fits: a multiple of
 # the far-field DFT's time block, short against the fits' duration
 AHEAD_STEPS = 48
+# longest wait for one checkpoint's fits in the pool (a fit takes about 60 ms)
+FIT_TIMEOUT_S = 600.0
 
 
 def start_fit_pool(workers: int | None = None) -> None:
@@ -785,7 +787,9 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                 if pool is not None:
                     # the refinement's Levenberg-Marquardt loop is Python: worker
                     # processes (one BLAS thread each) run the fits side by side
-                    fits = pool.map(_fit_job, jobs, chunksize=max(1, len(jobs) // (4 * _FIT_WORKERS)))
+                    # bounded: a worker that dies leaves map() waiting for good
+                    fits = pool.map_async(_fit_job, jobs, chunksize=max(1, len(jobs) // (4 * _FIT_WORKERS))
+                                          ).get(timeout=FIT_TIMEOUT_S)
                 else:
                     # LAPACK-bound fits release the GIL: one thread per host core,
                     # each with a single BLAS thread
