@@ -137,13 +137,18 @@ def evaluate_plain(ES, probs, ref, tiling, traces_out, group=128):
     np.savez_compressed(traces_out, V=np.array(V32), I=np.array(I32), dt=np.array(dts), ref=ref)
 
 
-def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out=None):
-    """Plain FP64 reference vs the early-stopped FP32 runs (with and without the network)."""
+def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out=None,
+             methods=("learned", "no_network", "pencil_rule"), plain_f32=True, subsets=None):
+    """Plain FP64 reference vs the early-stopped FP32 runs (with and without
+    the network) and, with plain_f32, plain FP32 runs of the full step count.
+    subsets: {name: run indices} reported separately for every method."""
     from special_topics_b200.backend import Batch, Engine
     freqs = ES.S11_FREQS
     out = {"plain_f64": {"time_s": t_plain, "steps": policy.n_total * len(probs)}}
-    for name, use_net, pol in (("learned", True, policy), ("no_network", False, policy),
-                               ("pencil_rule", False, ES.StopPolicy.refined(vp=False))):
+    rules = {"learned": (True, policy), "no_network": (False, policy),
+             "pencil_rule": (False, ES.StopPolicy.refined(vp=False))}
+    for name in methods:
+        use_net, pol = rules[name]
         errs, stops, winners, t = [], [], [], 0.0
         for g0 in range(0, len(probs), group):
             engs = [Engine(p, "f32-table") for p in probs[g0:g0 + group]]
@@ -166,6 +171,15 @@ def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out
                      "max_err_dB_p90": float(np.percentile(errs, 90)), "max_err_dB_worst": float(errs.max()),
                      "stops": {str(c): int(np.sum(np.array(stops) == c)) for c in sorted(set(stops))},
                      "winners": {w: winners.count(w) for w in set(winners)}}
+        for sub, idx in (subsets or {}).items():
+            e, st = errs[idx], np.array(stops)[idx]
+            out[name][sub] = {"runs": len(idx), "within_0p1_dB": float(np.mean(e <= 0.1)),
+                              "max_err_dB_worst": float(e.max()), "mean_stop_step": float(st.mean())}
+    if not plain_f32:
+        out["runs"] = len(probs)
+        if "learned" in out:
+            out["time_to_s11_ratio_plain_over_learned"] = out["plain_f64"]["time_s"] / out["learned"]["time_s"]
+        return out
     # plain FP32 runs of the full step count, for context (no early stop); their
     # traces (saved to traces_out) let other stop rules be replayed offline
     errs, t = [], 0.0
@@ -193,8 +207,8 @@ def evaluate(ES, probs, ref, t_plain, net, policy, tiling, group=128, traces_out
     errs = np.array(errs)
     out["plain_f32"] = {"time_s": t, "within_0p1_dB": float(np.mean(errs <= 0.1)),
                         "max_err_dB_median": float(np.median(errs)), "max_err_dB_worst": float(errs.max())}
-    out["time_to_s11_ratio_plain_over_learned"] = out["plain_f64"]["time_s"] / out["learned"]["time_s"]
-    out["time_to_s11_ratio_plain_over_no_network"] = out["plain_f64"]["time_s"] / out["no_network"]["time_s"]
+    for name in methods:
+        out[f"time_to_s11_ratio_plain_over_{name}"] = out["plain_f64"]["time_s"] / out[name]["time_s"]
     out["runs"] = len(probs)
     return out
 
@@ -213,6 +227,9 @@ def main():
                     help="also write the held-out runs' FP32 traces (es_test_traces.npz, about 110 KB per run) "
                          "for replaying stop rules offline")
     ap.add_argument("--no-eval", action="store_true", help="train and save only")
+    ap.add_argument("--eval-only", default=None, metavar="WEIGHTS",
+                    help="no training: evaluate these weights on the held-out seeds (learned rule and the "
+                         "pencil rule against plain FP64), the tuned and untouched halves reported apart")
     ap.add_argument("--shape", default="16,4,1,0,0",
                     help="batch launch shape chunk,rows,prefetch,group,streams (backend.Batch.set_tiling)")
     args = ap.parse_args()
@@ -231,6 +248,25 @@ def main():
     test_seeds = range(10000, 10000 + args.test)
     test_probs = ES.variant_problems(test_seeds, policy.n_total, pool)
     log(f"{len(test_probs)} test problems built")
+    if args.eval_only:
+        ref, t_plain = plain_reference(ES, pool, test_seeds, policy, tiling)
+        log("plain FP64 reference done")
+        pool.close()
+        net = ES.EsNet.load(args.eval_only, max_batch=128)
+        ES.start_fit_pool()
+        # the stop rule's thresholds were chosen on seeds 10000..10255
+        seeds = np.array(list(test_seeds))
+        subsets = {"seeds_10000_10255": np.flatnonzero(seeds < 10256).tolist(),
+                   "seeds_10256_up": np.flatnonzero(seeds >= 10256).tolist()}
+        metrics["weights"] = os.path.basename(args.eval_only)
+        metrics["evaluation"] = evaluate(ES, test_probs, ref, t_plain, net, policy, tiling,
+                                         methods=("learned", "pencil_rule"), plain_f32=False, subsets=subsets)
+        ES.stop_fit_pool()
+        net.close()
+        with open(os.path.join(args.out, "es_eval_metrics.json"), "w") as f:
+            json.dump(metrics, f, indent=1)
+        print(json.dumps(metrics["evaluation"]), flush=True)
+        return
     if args.cache and os.path.exists(args.cache):
         z = np.load(args.cache)
         x, y, ref, t_plain = z["x"], z["y"], z["ref"], float(z["t_plain"])
