@@ -1,4 +1,4 @@
-"""The early-stop driver's host logic (earlystop.run_with_early_stop) on the
+"""The early-stop checkpoint loop's host logic (earlystop.run_with_early_stop) on the
 CPU, with engines and batches faked: runs stop at the checkpoint where their
 fit passes, the runs left are re-batched and stepped on, the step-ahead
 during a checkpoint's fits ends soon after the fits return (in
@@ -90,7 +90,7 @@ def fake_batches(monkeypatch):
     return FakeBatch.log
 
 
-def test_driver_stops_rebatches_and_cuts_the_step_ahead_short(fake_batches):
+def test_checkpoint_loop_stops_rebatches_and_cuts_the_step_ahead_short(fake_batches):
     noisy = [False, True, False, True, False]
     traces = [_trace(q, z) for q, z in enumerate(noisy)]
     engs = [FakeEngine(V, I) for V, I in traces]
@@ -115,7 +115,7 @@ def test_driver_stops_rebatches_and_cuts_the_step_ahead_short(fake_batches):
     assert all(engs[q].step <= 70 + sum(ahead) for q in range(5) if not noisy[q])
 
 
-def test_driver_without_stops_reaches_the_end_as_plain_runs(fake_batches):
+def test_checkpoint_loop_without_stops_reaches_the_end_as_plain_runs(fake_batches):
     traces = [_trace(10 + q, True) for q in range(3)]
     engs = [FakeEngine(V, I) for V, I in traces]
     policy = ES.StopPolicy(n_in=40, checkpoints=(70, 250), n_total=N_TOTAL, pencil_orders=(4, 6, 8), decim=1,

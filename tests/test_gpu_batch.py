@@ -279,8 +279,8 @@ def test_member_mode_watchdog_and_profile():
             e.close()
 
 
-def test_early_stop_driver_keeps_each_runs_own_traces():
-    """The checkpoint driver steps the batch to the next checkpoint while it
+def test_early_stop_checkpoint_loop_keeps_each_runs_own_traces():
+    """The checkpoint loop steps the batch to the next checkpoint while it
     fits the current one, and rebuilds the batch when runs stop: every run's
     traces up to its stop step are still those of the same run stepped alone."""
     from special_topics_b200 import earlystop as ES
