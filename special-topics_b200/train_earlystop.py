@@ -231,7 +231,8 @@ def main():
                     help="no training: evaluate these weights on the held-out seeds (learned rule and the "
                          "pencil rule against plain FP64), the tuned and untouched halves reported apart")
     ap.add_argument("--shape", default="16,4,1,0,0",
-                    help="batch launch shape chunk,rows,prefetch,group,streams (backend.Batch.set_tiling)")
+                    help="batch launch shape chunk,rows,prefetch,group,streams[,width] (backend.Batch.set_tiling); "
+                         "64,16,1,0,0,16 is the batch tuner's shape for the variants")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     # one BLAS thread per pool worker (inherited by the spawned processes)
@@ -242,7 +243,8 @@ def main():
     _package()
     from special_topics_b200 import earlystop as ES
     policy = ES.StopPolicy.refined(max_resid=args.max_resid)
-    tiling = dict(zip(("chunk", "rows", "prefetch", "group", "streams"), (int(v) for v in args.shape.split(","))))
+    tiling = dict(zip(("chunk", "rows", "prefetch", "group", "streams", "width"),
+                      (int(v) for v in args.shape.split(","))))
     metrics = {"policy": policy.__dict__, "arch": ES.ARCH}
     t0 = time.perf_counter()
     test_seeds = range(10000, 10000 + args.test)
