@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import multiprocessing as mp
 import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
@@ -708,7 +709,6 @@ def start_fit_pool(workers: int | None = None) -> None:
     global _FIT_POOL, _FIT_WORKERS
     if _FIT_POOL is not None:
         return
-    import multiprocessing as mp
     import runpy
     _FIT_WORKERS = workers or min(16, os.cpu_count() or 1)
     boot = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_fit_worker.py")
@@ -716,12 +716,17 @@ def start_fit_pool(workers: int | None = None) -> None:
     _FIT_POOL.map(_warm_worker, range(_FIT_WORKERS), chunksize=1)   # every worker imports its modules now
 
 
-def stop_fit_pool() -> None:
+def stop_fit_pool(terminate: bool = False) -> None:
+    """Ends the fit pool (the fits then run in threads again); terminate=True
+    kills its workers instead of waiting for them."""
     global _FIT_POOL
     if _FIT_POOL is not None:
-        _FIT_POOL.close()
-        _FIT_POOL.join()
-        _FIT_POOL = None
+        pool, _FIT_POOL = _FIT_POOL, None
+        if terminate:
+            pool.terminate()
+        else:
+            pool.close()
+        pool.join()
 
 
 def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: dict | None = None,
@@ -788,8 +793,13 @@ def run_with_early_stop(engines, net: EsNet | None, policy: StopPolicy, tiling: 
                     # the refinement's Levenberg-Marquardt loop is Python: worker
                     # processes (one BLAS thread each) run the fits side by side
                     # bounded: a worker that dies leaves map() waiting for good
-                    fits = pool.map_async(_fit_job, jobs, chunksize=max(1, len(jobs) // (4 * _FIT_WORKERS))
-                                          ).get(timeout=FIT_TIMEOUT_S)
+                    try:
+                        fits = pool.map_async(_fit_job, jobs, chunksize=max(1, len(jobs) // (4 * _FIT_WORKERS))
+                                              ).get(timeout=FIT_TIMEOUT_S)
+                    except mp.TimeoutError:
+                        stop_fit_pool(terminate=True)
+                        raise RuntimeError(f"the stop fits of checkpoint {cp} did not finish in {FIT_TIMEOUT_S:.0f} s; "
+                                           "the fit pool was stopped") from None
                 else:
                     # LAPACK-bound fits release the GIL: one thread per host core,
                     # each with a single BLAS thread

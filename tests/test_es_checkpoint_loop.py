@@ -125,3 +125,36 @@ def test_checkpoint_loop_without_stops_reaches_the_end_as_plain_runs(fake_batche
         assert r["stopped_at"] == N_TOTAL and r["winner"] == "full run"
         assert np.array_equal(r["V"], traces[q][0]) and np.array_equal(r["I"], traces[q][1])
     assert all(e.step == N_TOTAL for e in engs)
+
+
+class StuckPool:
+    """A fit pool whose fits never return."""
+    terminated = False
+
+    def map_async(self, fn, jobs, chunksize=1):
+        class Never:
+            def get(self, timeout=None):
+                import multiprocessing as mp
+                raise mp.TimeoutError()
+        return Never()
+
+    def terminate(self):
+        StuckPool.terminated = True
+
+    def close(self):
+        pass
+
+    def join(self):
+        pass
+
+
+def test_stuck_fit_pool_ends_with_an_error_and_falls_back_to_threads(fake_batches, monkeypatch):
+    monkeypatch.setattr(ES, "_FIT_POOL", StuckPool())
+    engs = [FakeEngine(*_trace(q, False)) for q in range(2)]
+    policy = ES.StopPolicy(n_in=40, checkpoints=(70, 250), n_total=N_TOTAL, pencil_orders=(4, 6, 8), decim=1,
+                           max_resid=1e-6, agree_db=1e9, vp=True)
+    with pytest.raises(RuntimeError, match="did not finish"):
+        ES.run_with_early_stop(engs, None, policy, None, use_network=False)
+    assert StuckPool.terminated and ES._FIT_POOL is None
+    # the step-ahead started during the fits has ended with them
+    assert all(e.step <= 70 + ES.AHEAD_STEPS for e in engs)
