@@ -158,3 +158,24 @@ def test_stuck_fit_pool_ends_with_an_error_and_falls_back_to_threads(fake_batche
     assert StuckPool.terminated and ES._FIT_POOL is None
     # the step-ahead started during the fits has ended with them
     assert all(e.step <= 70 + ES.AHEAD_STEPS for e in engs)
+
+
+def test_fit_pool_and_threads_give_the_same_stops(fake_batches):
+    """The refined rule's fits in the spawned pool (as the bench runs them)
+    against the same fits in threads of this process."""
+    noisy = [False, True, False]
+    traces = [_trace(20 + q, z) for q, z in enumerate(noisy)]
+    policy = ES.StopPolicy(n_in=40, checkpoints=(70, 250, 330), n_total=N_TOTAL, pencil_orders=(4, 6, 8),
+                           decim=1, max_resid=1e-6, agree_db=1e9, vp=True, vp_decim=1)
+    out = {}
+    for name in ("threads", "pool"):
+        if name == "pool":
+            ES.start_fit_pool(2)
+        try:
+            engs = [FakeEngine(V, I) for V, I in traces]
+            out[name] = ES.run_with_early_stop(engs, None, policy, None, use_network=False)
+        finally:
+            ES.stop_fit_pool()
+    for a, b in zip(out["threads"], out["pool"]):
+        assert a["stopped_at"] == b["stopped_at"] and a["winner"] == b["winner"]
+        assert np.array_equal(a["V"], b["V"]) and np.array_equal(a["I"], b["I"])
