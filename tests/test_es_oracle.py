@@ -196,11 +196,18 @@ def test_fit_pool_gives_the_in_process_fits():
     pol = ES.StopPolicy.refined(pencil_orders=(4, 4, 4), vp_poles=2)
     modes = [complex(m1.s().real * 1.2, m1.s().imag * 1.01), complex(m2.s().real * 0.8, m2.s().imag * 0.99)]
     jobs = [(V[:cp], I[:cp], cp, dt, pol, None, False, modes) for cp in (2300, 3000)]
+    from threadpoolctl import threadpool_info
     ES.start_fit_pool(2)
     try:
         got = ES._FIT_POOL.map(ES._fit_job, jobs)
+        # every worker's BLAS libraries (NumPy's and SciPy's) run one thread:
+        # workers of one BLAS thread per core each slowed the fits 10-40x
+        infos = [ES._FIT_POOL.apply_async(threadpool_info).get(timeout=60) for _ in range(4)]
     finally:
         ES.stop_fit_pool()
+    for info in infos:
+        blas = [d for d in info if d["user_api"] == "blas"]
+        assert blas and all(d["num_threads"] == 1 for d in blas), blas
     for job, g in zip(jobs, got):
         want = ES._fit_job(job)
         assert (g is None) == (want is None)
