@@ -233,9 +233,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     workload = f"scaling-box-{args.grid}"
+    # bytes one half-step kernel streams per cell (fields, coefficients or ids)
+    half_step_bytes = int(np.prod(n)) * {"f32-table": 40, "f32": 72, "f64": 144}[args.precision]
+    l2 = ("inputs larger than L2 (fields and ids >> 126 MB), no flush needed" if half_step_bytes > 4 * L2_BYTES else
+          f"working set about {half_step_bytes / 2**20:.0f} MB per half-step against the 126 MB L2: partly "
+          "L2-resident, not an HBM figure")
     config = {"workload": workload, "grid": list(n), "cells": int(np.prod(n)), "ncpml": args.ncpml,
-              "far_field_freqs": 2,
-              "l2": "inputs larger than L2 (fields and ids >> 126 MB), no flush needed",
+              "far_field_freqs": 2, "l2": l2,
               "parallelism": f"{args.gpus} independent problem(s), one per GPU"}
 
     if args.cpu_sweep:
