@@ -52,3 +52,52 @@ def test_bad_arguments_are_rejected_with_a_message():
     assert rc == N.FDTD_ERR_BADARG
     assert b"too small" in L.fdtd_last_error()
     assert L.fdtd_run_batch(0, 1, None, None) == N.FDTD_ERR_STATE
+
+
+HANDLE_TYPES = ("fdtd_ctx", "fdtd_batch", "fdtd_es")
+
+
+def _handle_functions():
+    """Header entry points whose first parameter is a handle (or the member
+    list of fdtd_batch_create), with their return types."""
+    src = open(os.path.join(ROOT, "include", "fdtd_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for ret, name, args in re.findall(r"\b(int|void|double)\s+(fdtd_\w+)\s*\(([^)]*)\)", src):
+        first = args.split(",")[0]
+        if any(t in first for t in HANDLE_TYPES):
+            out[name] = ret
+    return out
+
+
+def _null_args(fn):
+    args = []
+    for t in fn.argtypes or []:
+        if t in (ctypes.c_int, ctypes.c_long, ctypes.c_longlong, ctypes.c_uint, ctypes.c_size_t):
+            args.append(0)
+        elif t in (ctypes.c_float, ctypes.c_double):
+            args.append(0.0)
+        else:
+            args.append(None)       # every pointer, the handle included
+    return args
+
+
+def test_null_handles_are_rejected_with_a_message():
+    """Every entry point that takes a handle answers a NULL handle (and NULL
+    pointers) with an error code and a message, as the reference's ABI does
+    (FDTD_OK / FDTD_ERR, fdtd_last_error: fdtd_cuda.h:12-13, fdtd_cuda.cu:40-41),
+    before any device work: no GPU is needed for any of these calls."""
+    L = N.lib()
+    funcs = _handle_functions()
+    assert len(funcs) >= 50
+    for name, ret in sorted(funcs.items()):
+        fn = getattr(L, name)
+        assert fn.argtypes is not None, f"{name} has no argtypes in _native"
+        rc = fn(*_null_args(fn))
+        if ret == "void":
+            continue                                   # the free functions accept NULL
+        if name in ("fdtd_ctx_step", "fdtd_batch_size"):
+            assert rc == -1, name
+            continue
+        assert rc == N.FDTD_ERR_BADARG, f"{name} returned {rc}"
+        assert L.fdtd_last_error(), name
